@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""Benchmark of the PDHG hot path on the config-2 LP (m=1e6, n=2e6, 20M nnz,
+power-law rows), one B200.
+
+A *step* is one check interval of the reference's driver: 100 PDHG trials
+(IterationBackend::advance(100, tau, sigma), src/solver.cpp:524-526).  The
+metric is the SpMV HBM bandwidth of those trials: the algorithmic bytes of the
+two SpMVs of one PDHG iteration (A^T y and A dx,
+nnz*(s_v+s_i) + (rows+1)*s_p + cols*8 + rows*8 each) times iterations per
+second.  The instance (synthetic, seeded) is larger than L2 (about 730 MB of
+traffic per iteration), so no L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl nk|reference]
+
+Multi-GPU: a single LP is not partitioned (replicas only); each rank runs its
+own replica and `value` is the sum over ranks of the work done in the max-over-
+ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "SpMV HBM GB/s"
+TRIALS_PER_STEP = 100
+
+
+def spmv_bytes(rows, cols, nnz, s_v=8, s_i=4, s_p=4):
+    """Algorithmic bytes of one CSR SpMV: matrix once, input vector once, output once."""
+    return nnz * (s_v + s_i) + (rows + 1) * s_p + cols * 8 + rows * 8
+
+
+def iteration_spmv_bytes(m, n, nnz, s_v=8):
+    return spmv_bytes(m, n, nnz, s_v) + spmv_bytes(n, m, nnz, s_v)
+
+
+def fused_kernel_bytes(m, n, nnz, s_v=8):
+    """Algorithmic bytes of the two fused kernels of one trial.
+    primal: A^T (nnz, n+1 ptr) + gather y (m) + read x, c, q, lb, ub, xa + write trial, dx, xa (n)
+    dual:   A (nnz, m+1 ptr) + gather dx (n) + read y, Ax, rl, ru, ya + write trial, Ax', ya (m)"""
+    primal = nnz * (s_v + 4) + (n + 1) * 4 + m * 8 + 9 * 8 * n
+    dual = nnz * (s_v + 4) + (m + 1) * 4 + n * 8 + 8 * 8 * m
+    return primal, dual
+
+
+def step_sizes(model):
+    """Step and primal weight exactly as solve_continuous initialises them
+    (src/solver.cpp:299-333): step = 0.9/sqrt(max row l1 * max col l1),
+    weight = clamp(||c|| / ||clamp(0, rl, ru)||, 1e-4, 1e4)."""
+    a = np.abs(model.val)
+    rows = np.add.reduceat(a, model.ptr[:-1]) if model.nnz else np.zeros(model.m)
+    rows[np.diff(model.ptr) == 0] = 0
+    cols = np.bincount(model.idx, weights=a, minlength=model.n)
+    norm = math.sqrt(rows.max()) * math.sqrt(cols.max())
+    step = 0.9 / norm if norm > 0 else 1.0
+    c2 = float(np.dot(model.c, model.c))
+    b = np.clip(0.0, model.rl, model.ru)
+    b2 = float(np.dot(b, b))
+    weight = min(1e4, max(1e-4, math.sqrt(c2 / b2))) if c2 > 1e-24 and b2 > 1e-24 else 1.0
+    return step / weight, step * weight
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (clocks and throttle reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index=0):
+        self.idx = device_index
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.file:
+            return None
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def build_model(args):
+    from niryukti_b200 import synth
+    if args.small:
+        return synth.power_law_lp(m=100_000, n=200_000, nnz=2_000_000, seed=2)
+    return synth.power_law_lp(seed=2)
+
+
+# ---------------------------------------------------------------- CPU arm
+def cpu_rate(model, seconds, threads, trials_per_sample):
+    """The reference's CpuBackend (oracle/_ref, the reference's own code) when built,
+    else the C oracle port: PDHG iterations/s on the same instance."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle import oracle as orc
+    kind = "reference" if orc.REF_SO.exists() else "port"
+    if kind == "reference":
+        be = orc.Reference().model(model).backend(np.zeros(model.n), np.zeros(model.m),
+                                                  adaptive=True)
+    else:
+        be = orc.Oracle().model(model).backend(np.zeros(model.n), np.zeros(model.m),
+                                               adaptive=True)
+        threads = 1
+    tau, sigma = step_sizes(model)
+    be.advance(1, tau, sigma)  # warm caches
+    done, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        done += be.advance(trials_per_sample, tau, sigma)
+    dt = time.perf_counter() - t0
+    return done / dt, kind, threads, done, dt
+
+
+def cpu_child(args):
+    model = build_model(args)
+    rate, kind, threads, done, dt = cpu_rate(model, args.cpu_seconds, args.cpu_threads,
+                                            args.cpu_trials)
+    print(json.dumps({"rate": rate, "kind": kind, "threads": threads, "done": done, "dt": dt}))
+
+
+def run_cpu_child(args):
+    cmd = [sys.executable, str(pathlib.Path(__file__).resolve()), "--cpu-child",
+           "--cpu-seconds", str(args.cpu_seconds), "--cpu-threads", str(args.cpu_threads),
+           "--cpu-trials", str(args.cpu_trials)] + (["--small"] if args.small else [])
+    env = dict(os.environ, OMP_NUM_THREADS=str(args.cpu_threads))
+    out = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=1800)
+    if out.returncode != 0:
+        raise RuntimeError(out.stderr[-2000:])
+    return json.loads(out.stdout.strip().splitlines()[-1])
+
+
+def reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    model = build_model(args)
+    m, n, nnz = model.m, model.n, model.nnz
+    threads = args.cpu_threads
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle import oracle as orc
+    kind = "reference" if orc.REF_SO.exists() else "port"
+    if kind == "reference":
+        be = orc.Reference().model(model).backend(np.zeros(n), np.zeros(m), adaptive=True)
+    else:
+        be = orc.Oracle().model(model).backend(np.zeros(n), np.zeros(m), adaptive=True)
+        threads = 1
+    tau, sigma = step_sizes(model)
+    per = args.ref_trials
+    for _ in range(args.warmup):
+        be.advance(per, tau, sigma)
+    t0 = time.perf_counter()
+    done = 0
+    for _ in range(args.steps):
+        done += be.advance(per, tau, sigma)
+    dt = time.perf_counter() - t0
+    rate = done / dt
+    value = rate * iteration_spmv_bytes(m, n, nnz) / 1e9
+    line = {"metric": METRIC, "value": value, "unit": "GB/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "config2_power_law_lp_m1e6_n2e6_nnz2e7", "m": m, "n": n,
+                       "nnz": nnz, "trials_per_step": per, "seed": 2},
+            "iterations_per_s": rate,
+            "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": kind,
+                             "sample": f"{args.steps} steps x {per} PDHG trials of the "
+                                       "config-2 LP (adaptive, FP64), CpuBackend::advance"},
+            "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------- engine arm
+def engine_arm(args, world, rank, local):
+    import torch
+    from niryukti_b200 import engine
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    model = build_model(args)
+    m, n, nnz = model.m, model.n, model.nnz
+    tau, sigma = step_sizes(model)
+    g = engine.PdhgBackend(model, adaptive=True, graphs=True, precision=args.precision)
+    sched = g.schedule_info()
+    ext = torch.cuda.ExternalStream(g.stream())
+    s_v = 8 if args.precision == "fp64" else 4
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        g.advance(TRIALS_PER_STEP, tau, sigma)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = Clocks(local)
+    with clocks:
+        e0.record(ext)
+        accepted = 0
+        for _ in range(args.steps):
+            accepted += g.advance(TRIALS_PER_STEP, tau, sigma)
+        e1.record(ext)
+        e1.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    trials = args.steps * TRIALS_PER_STEP
+    it_s = trials / (ms / 1e3)
+    value = world * it_s * iteration_spmv_bytes(m, n, nnz, s_v) / 1e9
+
+    # per-kernel durations (CUDA events around each kernel, same stream)
+    ms_p, ms_d = g.profile(args.profile_trials, tau, sigma)
+    bp, bd = fused_kernel_bytes(m, n, nnz, s_v)
+    kernels = {"primal_kernel": {"ms": ms_p, "bytes": bp, "GBps": bp / ms_p / 1e6},
+               "dual_kernel": {"ms": ms_d, "bytes": bd, "GBps": bd / ms_d / 1e6}}
+    top = max(kernels, key=lambda k: kernels[k]["ms"])
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    roofline = {"bound": "hbm", "kernel": top, "achieved": kernels[top]["GBps"], "peak": peak,
+                "unit": "GB/s", "frac": kernels[top]["GBps"] / peak, "traffic": args.traffic,
+                "peak_source": "measured" if pk.exists() else "fallback"}
+
+    # e2e through the C ABI with host buffers: per step upload (x, y), 100 trials,
+    # download the four candidates -- the reference driver's per-check pattern
+    hx = torch.zeros(n, dtype=torch.float64).pin_memory()
+    hy = torch.zeros(m, dtype=torch.float64).pin_memory()
+    outs = [torch.empty(k, dtype=torch.float64).pin_memory() for k in (n, m, n, m)]
+    hxn, hyn = hx.numpy(), hy.numpy()
+    on = [o.numpy() for o in outs]
+    cx, cy, cxa, cya = g.candidates()
+    hxn[:] = cx
+    hyn[:] = cy
+    barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(ext)
+    w0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        g.reset(hxn, hyn)
+        g.advance(TRIALS_PER_STEP, tau, sigma)
+        res = g.candidates()
+        for dst, src in zip(on, res):
+            dst[:] = src
+    f1.record(ext)
+    f1.synchronize()
+    wall = time.perf_counter() - w0
+    e2e_ms = max(f0.elapsed_time(f1), 1e3 * wall)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * (args.e2e_steps * TRIALS_PER_STEP / (e2e_ms / 1e3)) * \
+        iteration_spmv_bytes(m, n, nnz, s_v) / 1e9
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    cpu = None
+    if not args.no_cpu:
+        try:
+            c = run_cpu_child(args)
+            cpu = {"value": c["rate"] * iteration_spmv_bytes(m, n, nnz) / 1e9, "unit": "GB/s",
+                   "cores": c["threads"], "kind": c["kind"],
+                   "sample": f"{c['done']} adaptive FP64 PDHG trials of the same config-2 LP in "
+                             f"{c['dt']:.1f} s (CpuBackend::advance, OMP threads {c['threads']})",
+                   "iterations_per_s": c["rate"]}
+        except Exception as exc:  # reported, never silently replaced
+            cpu = {"error": str(exc)[-500:]}
+    line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32-matrix/f64-iterates",
+            "data": "synthetic (seeded power-law LP, numpy PCG64 seed 2)",
+            "config": {"workload": "config2_power_law_lp_m1e6_n2e6_nnz2e7" if not args.small
+                       else "config2_small", "m": m, "n": n, "nnz": nnz,
+                       "trials_per_step": TRIALS_PER_STEP, "precision": args.precision,
+                       "adaptive": True, "graphs": True, "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (about 730 MB per iteration)"},
+            "iterations_per_s": it_s,
+            "whole_iteration_GBps": it_s * sum(fused_kernel_bytes(m, n, nnz, s_v)) / 1e9,
+            "kernels": kernels, "schedule": sched, "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "GB/s",
+                    "h2d_bytes_per_step": 8 * (n + m), "d2h_bytes_per_step": 16 * (n + m),
+                    "path": "nk_pdhg_reset + nk_pdhg_advance(100) + nk_pdhg_candidates"},
+            "gpu_launches": 2 * (args.steps * TRIALS_PER_STEP),
+            "clocks": clocks.summary(), "accepted_trials": accepted}
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="nk", choices=["nk", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "fp32"])
+    ap.add_argument("--small", action="store_true", help="10x smaller instance (testing)")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-child", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-threads", type=int, default=os.cpu_count() or 1)
+    ap.add_argument("--cpu-trials", type=int, default=5)
+    ap.add_argument("--ref-trials", type=int, default=10)
+    ap.add_argument("--profile-trials", type=int, default=20)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--traffic", type=float, default=None,
+                    help="DRAM bytes per launch of the top kernel from an ncu capture")
+    args = ap.parse_args()
+    if args.warmup < 3 and not args.cpu_child:
+        ap.error("--warmup must be at least 3")
+    if args.cpu_child:
+        return cpu_child(args)
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        return reference_arm(args, world, rank)
+    return engine_arm(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

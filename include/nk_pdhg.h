@@ -1,0 +1,141 @@
+/* nk_pdhg.h -- C ABI of the B200 PDHG engine (libnkpdhg.so).
+ *
+ * The engine replaces the reference's CUDA iteration backend: every function of
+ * the nk_pdhg_* family implements one member of the reference's plugin
+ * interface `IterationBackend` (src/internal.hpp:102-124) and its factory
+ * `cuda_backend()` (src/internal.hpp:129-134), with the semantics of the
+ * reference's CUDA implementation `CudaBackend` (src/cuda.cu:565-950).  The
+ * C++ adapter that plugs these calls into the reference's host code lives in
+ * niryukti_b200/bridge/vantage_cuda_bridge.cpp.
+ *
+ * Conventions (mirroring the reference's C API, src/c_api.cpp:11-37):
+ *   - every call returns an nk_status; on failure nk_last_error() holds a
+ *     thread-local message; no C++ exception crosses this boundary;
+ *   - the caller owns every host array; the engine copies what it keeps;
+ *   - a handle is single-threaded (one CUDA stream); distinct handles may be
+ *     used concurrently from different threads;
+ *   - matrices arrive in the reference's CSR layout (int64 ptr/index, double
+ *     values, src/model.cpp:11-38), canonical: rows sorted, columns strictly
+ *     increasing inside a row.
+ */
+#ifndef NK_PDHG_H
+#define NK_PDHG_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    NK_OK = 0,
+    NK_ERR_INVALID = 1,     /* bad argument or inconsistent model */
+    NK_ERR_CUDA = 2,        /* CUDA runtime failure */
+    NK_ERR_MEMORY = 3,      /* device memory guard or allocation failure */
+    NK_ERR_STALLED = 4,     /* backtracking stalled / non-finite fixed step */
+    NK_ERR_UNSUPPORTED = 5, /* option combination the engine refuses */
+    NK_ERR_NO_DEVICE = 6    /* no CUDA device visible */
+} nk_status;
+
+/* CSR matrix in host memory, reference layout (vantage::Sparse,
+ * include/vantage/vantage.hpp:17-24). */
+typedef struct {
+    int64_t rows, cols;
+    const int64_t *ptr;   /* rows + 1 */
+    const int64_t *index; /* ptr[rows] */
+    const double *value;  /* ptr[rows] */
+} nk_csr;
+
+/* Matrix precisions (the reference's --matrix-precision, src/cuda.cu:117-160). */
+#define NK_PRECISION_FP64 0  /* FP64 values, FP64 accumulation */
+#define NK_PRECISION_MIXED 1 /* FP32 values, FP64 vectors and accumulation (reference "mixed") */
+#define NK_PRECISION_FP32 2  /* FP32 values, FP32 gathered vectors and FP32 accumulation;
+                                iterates, averages, reductions and control stay FP64 */
+
+/* Options of cuda_backend() (src/internal.hpp:129-134). */
+typedef struct {
+    int adaptive;          /* adaptive step acceptance (src/cuda.cu:300-312) */
+    int halpern;           /* Halpern anchoring (src/cuda.cu:316-327) */
+    double reflection;     /* Halpern reflection in [0, 1] */
+    int residual_restarts; /* fixed-point residual restart requests */
+    int graphs;            /* replay trials from CUDA graphs */
+    int index_bits;        /* 0 = auto (32 when it fits), 32 or 64 (--gpu-indices) */
+    int precision;         /* NK_PRECISION_* */
+} nk_pdhg_options;
+
+typedef struct nk_pdhg nk_pdhg;
+
+/* cuda_backend(model, x, y, ...) -- src/internal.hpp:129-134, src/cuda.cu:1288-1303.
+ * A is m x n; Q (n x n, exactly symmetric) may be NULL or empty.  c, q, lb, ub
+ * have n entries, rl, ru m entries, x0 n and y0 m.  Applies the reference's
+ * memory guard ("Estimated GPU storage exceeds 80% of available memory"). */
+nk_status nk_pdhg_create(const nk_csr *A, const nk_csr *Q, const double *c, const double *q,
+                         const double *lb, const double *ub, const double *rl, const double *ru,
+                         const double *x0, const double *y0, const nk_pdhg_options *opts,
+                         nk_pdhg **out);
+void nk_pdhg_destroy(nk_pdhg *h);
+
+/* IterationBackend::advance(count, tau, sigma) -- src/internal.hpp:105,
+ * src/cuda.cu:816-866.  Runs `count` PDHG trials with base steps tau, sigma;
+ * *accepted receives the accepted progress.  Like the reference CUDA backend it
+ * fails with NK_ERR_STALLED after four chunks without progress, or when a
+ * fixed-step run produced a non-finite step. */
+nk_status nk_pdhg_advance(nk_pdhg *h, int count, double tau, double sigma, int *accepted);
+
+/* IterationBackend::rejected_steps / restart_requested -- src/internal.hpp:108-113. */
+nk_status nk_pdhg_rejected_steps(nk_pdhg *h, int64_t *out);
+nk_status nk_pdhg_restart_requested(nk_pdhg *h, int *out);
+
+/* IterationBackend::monitor -- src/internal.hpp:114-116, src/cuda.cu:657-738:
+ * scaled-space KKT proxy, min over the current and averaged points. */
+nk_status nk_pdhg_monitor(nk_pdhg *h, double *out);
+
+/* IterationBackend::candidates(x, y, xa, ya) -- src/internal.hpp:117-118,
+ * src/cuda.cu:867-891: copies the current and averaged iterates to the host
+ * arrays (n, m, n, m entries) and rebases the resident A*x. */
+nk_status nk_pdhg_candidates(nk_pdhg *h, double *x, double *y, double *xa, double *ya);
+
+/* IterationBackend::reset_candidate(average) -- src/internal.hpp:120-122,
+ * src/cuda.cu:892-930: restart from the resident current (0) or averaged (1)
+ * point without host uploads. */
+nk_status nk_pdhg_reset_candidate(nk_pdhg *h, int average);
+
+/* IterationBackend::reset(x, y) -- src/internal.hpp:123, src/cuda.cu:931-949. */
+nk_status nk_pdhg_reset(nk_pdhg *h, const double *x, const double *y);
+
+/* IterationBackend::snapshot / restore -- src/internal.hpp:106-107,
+ * src/cuda.cu:739-770.  The snapshot is a list of `parts` vectors; sizes first
+ * (nk_pdhg_snapshot_layout), then the flattened values.  restore() accepts only
+ * a snapshot of an engine of the same shape and options. */
+nk_status nk_pdhg_snapshot_layout(nk_pdhg *h, int *parts, int64_t *part_sizes /* >= 16 */);
+nk_status nk_pdhg_snapshot(nk_pdhg *h, double *out);
+nk_status nk_pdhg_restore(nk_pdhg *h, const double *in, const int64_t *part_sizes, int parts);
+
+/* Engine statistics for benchmarking: trials launched so far and the device
+ * memory the handle holds. */
+nk_status nk_pdhg_stats(nk_pdhg *h, int64_t *trials, int64_t *device_bytes);
+
+/* Profiling (no reference counterpart): runs `count` trials one at a time with
+ * CUDA events around each kernel on the engine's stream and returns the mean
+ * duration of the fused primal (A^T y + primal step) and dual (A dx + dual step
+ * + decision) kernels in milliseconds.  The trials advance the iterate. */
+nk_status nk_pdhg_profile(nk_pdhg *h, int count, double tau, double sigma, double *ms_primal,
+                          double *ms_dual);
+/* The CUDA stream (cudaStream_t) every kernel and copy of this handle runs on,
+ * for callers that time the engine with CUDA events. */
+nk_status nk_pdhg_stream(nk_pdhg *h, void **stream);
+/* Row schedule chosen for A and A^T: sub-warp width, long-row threshold, items. */
+nk_status nk_pdhg_schedule_info(nk_pdhg *h, int *a_width, int64_t *a_long, int *at_width,
+                                int64_t *at_long, int *a_items, int *at_items);
+
+/* cuda_available / cuda_description / hardware_info --
+ * include/vantage/vantage.hpp:76,145-146, src/cuda.cu:1267-1287. */
+int nk_cuda_available(void);
+nk_status nk_cuda_description(char *buffer, int length);
+nk_status nk_hardware_info(int *available, double *free_bytes, double *total_bytes);
+
+const char *nk_last_error(void);
+unsigned nk_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -68,12 +68,13 @@ class Model:
         return self.qnnz > 0 or bool(np.any(self.q != 0))
 
     def multiply(self, x: np.ndarray) -> np.ndarray:
-        """A @ x with the same row-sequential FP64 summation order as Sparse::multiply."""
+        """A @ x in FP64 (numpy's segment sums; the summation order is numpy's, so the
+        last bits can differ from the reference's row-sequential Sparse::multiply).
+        Used only to define instances (b = A x0), never as a parity check."""
         return csr_matvec(self.ptr, self.idx, self.val, x, self.m)
 
 
 def csr_matvec(ptr, idx, val, x, rows):
-    # numpy reduceat sums each segment left to right in FP64 for float64 input
     prod = val * x[idx]
     out = np.zeros(rows, dtype=np.float64)
     lens = np.diff(ptr)
