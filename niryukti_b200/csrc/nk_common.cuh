@@ -51,11 +51,18 @@ template <class T> struct DevBuf {
     size_t n = 0;
     DevBuf() = default;
     explicit DevBuf(size_t count) { alloc(count); }
+    // Every buffer carries kSlack zeroed bytes past its end: bulk copies widen
+    // their ranges to 16-byte boundaries and may read up to 15 bytes beyond.
+    static constexpr size_t kSlack = 64;
     void alloc(size_t count) {
         release();
         n = count;
-        if (count)
-            cuda_check(cudaMalloc(reinterpret_cast<void **>(&p), count * sizeof(T)), "cudaMalloc");
+        if (count) {
+            cuda_check(cudaMalloc(reinterpret_cast<void **>(&p), count * sizeof(T) + kSlack),
+                       "cudaMalloc");
+            cuda_check(cudaMemset(reinterpret_cast<char *>(p) + count * sizeof(T), 0, kSlack),
+                       "slack");
+        }
     }
     void release() noexcept {
         if (p)

@@ -1,23 +1,14 @@
-// B200 PDHG iteration engine: the replacement for the reference's CudaBackend
-// (src/cuda.cu:565-950) behind the IterationBackend seam (src/internal.hpp:102-134).
+// B200 PDHG iteration engine, host side: the replacement for the reference's
+// CudaBackend (src/cuda.cu:565-950) behind the IterationBackend seam
+// (src/internal.hpp:102-134), exported through the C ABI of include/nk_pdhg.h.
+// The kernels are in nk_device.cuh.
 //
-// One PDHG trial is two kernels:
-//   primal_kernel  g = c + A^T y (+ Q x + q.x)      -- CSR SpMV over the explicit transpose
-//                  trial x = clamp((x - tau g)/(1 + tau q), lb, ub), dx, sum dx^2
-//                  (restates primal_trial, src/cuda.cu:240-260, and the CPU loop
-//                   src/cpu.cpp:107-132, fused into the SpMV epilogue)
-//   dual_kernel    delta = A dx                      -- CSR SpMV
-//                  trial y = interval prox of y + sigma (Ax + 2 delta), Ax + delta,
-//                  sum dy^2, sum dy*delta            (dual_trial, src/cuda.cu:261-284;
-//                                                     src/cpu.cpp:136-150)
-//                  and, in its last CTA, the accept / step-factor / averaging decision
-//                  (decide, src/cuda.cu:285-335; src/cpu.cpp:151-216)
-// Iterates are double-buffered: accepting a trial flips a device-side index, and the
-// running-average update of an accepted step is applied by the next trial's kernels
-// (commit_primal / commit_dual, src/cuda.cu:336-370, without their own passes).
-// The Halpern variant keeps a separate commit kernel.
+// Engine order: the rows of A and the rows of A^T (the columns of A) are sorted
+// by length, longest first (stable), and stored as SELL-32 (nk_sell.cuh).  Every
+// vector lives on the device in that order; vectors are permuted on their way in
+// and out, so callers only ever see their own order.
 #include "nk_common.cuh"
-#include "nk_kernels.cuh"
+#include "nk_device.cuh"
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 #include <algorithm>
@@ -28,607 +19,332 @@
 #include <numeric>
 #include <vector>
 
+#ifndef NK_SPLIT
+#define NK_SPLIT 256 // rows with more entries are split into virtual rows of this length
+#endif
+
 namespace nk {
 
 thread_local char g_last_error[2048] = {};
 void set_last_error(const char *what) { std::snprintf(g_last_error, sizeof(g_last_error), "%s", what); }
 
-// Device-resident control state.  The first eleven fields keep the meaning of
-// the reference's `state` vector (src/cuda.cu:224-225,601).
-struct Control {
-    double factor;    // step multiplier
-    double mass;      // averaging mass
-    double accepted;  // accepted trials
-    double rejected;  // rejected trials
-    double accept;    // last trial accepted
-    double weight;    // last averaging weight
-    double epoch;     // Halpern epoch steps
-    double init_res;  // Halpern initial residual
-    double prev_res;  // Halpern previous residual
-    double restart;   // Halpern restart requested
-    double lambda;    // Halpern anchor weight
-    double tau, sigma;  // base steps of the current chunk (device-resident for graph replay)
-    double pending_w;   // averaging weight of the accepted step not yet folded in
-    int cur;            // which x / y / Ax buffer holds the current iterate
-    int pending;        // 1 while pending_w must still be applied
-    unsigned arrive;    // last-CTA detection in dual_kernel
-    int flags;          // bit 0 adaptive, bit 1 halpern, bit 2 residual restarts
-};
-
-struct Vecs {
-    const double *c, *q, *lb, *ub, *rl, *ru;
-    double *x0, *x1, *y0, *y1, *ax0, *ax1, *xa, *ya;
-    double *dx;        // primal displacement (FP64 gather source)
-    float *dx32;       // FP32 gather source (precision FP32)
-    float *y32_0, *y32_1; // FP32 copies of y (precision FP32)
-    double *anchor_x, *anchor_y, *anchor_ax;
-    double *part_p;    // per-CTA sum dx^2 of primal_kernel
-    double *part_d;    // per-CTA (sum dy^2, sum dy*delta) of dual_kernel
-    Control *ctl;
-    int grid_p;        // CTAs of primal_kernel (partials to read)
-    double reflection;
-};
-
-__device__ __forceinline__ double clampd(double v, double lo, double hi) {
-    return v < lo ? lo : (hi < v ? hi : v); // std::clamp
-}
-__device__ __forceinline__ double max0(double v) { return 0. < v ? v : 0.; } // std::max(0., v)
-__device__ __forceinline__ double min0(double v) { return v < 0. ? v : 0.; } // std::min(0., v)
-
-// ------------------------------------------------------------------ primal
-template <class Acc, class V, class P, class I, bool SPARSE_Q, bool FP32G>
-__global__ void __launch_bounds__(kThreads) primal_kernel(Csr<V, P, I> At, Schedule S,
-                                                          Csr<V, P, I> Q, Schedule /*unused*/,
-                                                          Vecs v) {
-    __shared__ double red[kWarps];
-    __shared__ Acc qred[kWarps];
-    const Control &ctl = *v.ctl;
-    double mine = 0;
-    bool bad = false;
-    if (ctl.restart == 0) {
-        const int cur = ctl.cur;
-        const bool pending = ctl.pending != 0;
-        const double pw = ctl.pending_w;
-        const double tau = ctl.tau * ctl.factor;
-        const double *x = cur ? v.x1 : v.x0;
-        double *xt = cur ? v.x0 : v.x1;
-        const double *y = cur ? v.y1 : v.y0;
-        const float *y32 = cur ? v.y32_1 : v.y32_0;
-        auto body = [&](int64_t j, Acc s, bool leader, bool valid, auto group, int lane) {
-            constexpr int G = decltype(group)::value;
-            Acc qs = Acc(0);
-            if constexpr (SPARSE_Q) {
-                if constexpr (G == kThreads)
-                    qs = cta_dot<Acc>(Q, j, x, qred);
-                else
-                    qs = group_dot<G, Acc>(Q, j, valid, x, lane);
-            }
-            if (!leader)
-                return;
-            double xj = x[j];
-            if (pending) {
-                double a = v.xa[j];
-                v.xa[j] = a + (xj - a) * pw;
-            }
-            double g = v.c[j] + double(s);
-            double qj = v.q[j];
-            if constexpr (SPARSE_Q)
-                g = g + (double(qs) + qj * xj);
-            double t = (xj - tau * g) / (1 + tau * (SPARSE_Q ? 0. : qj));
-            t = clampd(t, v.lb[j], v.ub[j]);
-            xt[j] = t;
-            double d = t - xj;
-            if constexpr (FP32G)
-                v.dx32[j] = float(d);
-            else
-                v.dx[j] = d;
-            mine += d * d;
-            bad |= !isfinite(t);
-        };
-        if constexpr (FP32G)
-            sweep<Acc>(At, S, y32, body);
-        else
-            sweep<Acc>(At, S, y, body);
-    }
-    double tot[1] = {bad ? INFINITY : mine};
-    cta_sum<1>(tot, red);
-    if (threadIdx.x == 0)
-        v.part_p[blockIdx.x] = tot[0];
-}
-
-// ------------------------------------------------------------------ dual + decide
-__device__ void decide(Vecs &v, double p, double d, double c) {
-    Control &s = *v.ctl;
-    const bool adaptive = s.flags & 1, halpern = s.flags & 2, residual_restarts = s.flags & 4;
-    if (s.restart != 0) { // a requested Halpern restart freezes the chunk (src/cuda.cu:298-301)
-        s.accept = 0;
-        return;
-    }
-    double factor = s.factor;
-    double tau = s.tau * factor, sigma = s.sigma * factor;
-    double energy = p / tau + d / sigma;
-    double limit = fabs(c) > 0 ? energy / (2 * fabs(c)) : INFINITY;
-    bool finite = isfinite(energy) && isfinite(c);
-    bool accept = finite && (!adaptive || limit >= 1);
-    if (adaptive) {
-        double k = s.accepted + 2;
-        double mult = fmin((1 - pow(k, -.3)) * limit, 1 + pow(k, -.6));
-        if (!finite || !isfinite(mult) || mult <= 0)
-            mult = .5;
-        s.factor = clampd(factor * mult, 1e-12, 1e12);
-    }
-    s.accept = accept ? 1 : 0;
-    s.pending = 0;
-    if (accept) {
-        s.mass += factor;
-        s.accepted += 1;
-        s.weight = factor / s.mass;
-        if (halpern) {
-            double residual = sqrt(fmax(0., energy - 2 * c));
-            if (s.epoch == 0)
-                s.init_res = residual;
-            s.lambda = 1 / (s.epoch + 2);
-            s.epoch += 1;
-            // integer halving as in the CPU backend (src/cpu.cpp:196)
-            double half = double(int64_t(s.accepted) / 2);
-            bool req = residual_restarts && s.epoch >= 10 &&
-                       (residual <= .2 * s.init_res ||
-                        (residual <= .8 * s.init_res && residual > s.prev_res) ||
-                        s.epoch >= fmax(10., half));
-            s.restart = req ? 1 : 0;
-            s.prev_res = residual;
-        } else {
-            s.cur ^= 1;
-            s.pending = 1;
-            s.pending_w = s.weight;
-        }
-    } else
-        s.rejected += 1;
-}
-
-template <class Acc, class V, class P, class I, bool FP32G>
-__global__ void __launch_bounds__(kThreads) dual_kernel(Csr<V, P, I> A, Schedule S, Vecs v) {
-    __shared__ double red[kWarps * 3];
-    __shared__ bool last;
-    const Control &ctl = *v.ctl;
-    double dy2 = 0, cpl = 0;
-    bool bad = false;
-    if (ctl.restart == 0) {
-        const int cur = ctl.cur;
-        const bool pending = ctl.pending != 0;
-        const double pw = ctl.pending_w;
-        const double sigma = ctl.sigma * ctl.factor;
-        const double *y = cur ? v.y1 : v.y0;
-        double *yt = cur ? v.y0 : v.y1;
-        float *yt32 = cur ? v.y32_0 : v.y32_1;
-        const double *ax = cur ? v.ax1 : v.ax0;
-        double *axt = cur ? v.ax0 : v.ax1;
-        auto body = [&](int64_t i, Acc s, bool leader, bool, auto, int) {
-            if (!leader)
-                return;
-            double yi = y[i], axi = ax[i];
-            if (pending) {
-                double a = v.ya[i];
-                v.ya[i] = a + (yi - a) * pw;
-            }
-            double delta = double(s);
-            double bar = axi + 2 * delta;
-            double z = yi + sigma * bar;
-            double t = max0(z - sigma * v.ru[i]) + min0(z - sigma * v.rl[i]);
-            yt[i] = t;
-            if constexpr (FP32G)
-                yt32[i] = float(t);
-            axt[i] = axi + delta;
-            double dy = t - yi;
-            dy2 += dy * dy;
-            cpl += dy * delta;
-            bad |= !isfinite(bar) || !isfinite(t) || !isfinite(delta);
-        };
-        if constexpr (FP32G)
-            sweep<Acc>(A, S, v.dx32, body);
-        else
-            sweep<Acc>(A, S, v.dx, body);
-    }
-    double tot[2] = {bad ? INFINITY : dy2, cpl};
-    cta_sum<2>(tot, red);
-    if (threadIdx.x == 0) {
-        v.part_d[2 * blockIdx.x] = tot[0];
-        v.part_d[2 * blockIdx.x + 1] = tot[1];
-        __threadfence();
-        unsigned prev = atomicAdd(&v.ctl->arrive, 1u);
-        last = prev == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!last)
-        return;
-    // Last CTA: every other CTA of this launch and the whole primal launch are
-    // complete; combine partials in index order (deterministic) and decide.
-    __threadfence();
-    double p = 0, d = 0, c = 0;
-    for (int b = threadIdx.x; b < v.grid_p; b += kThreads)
-        p += v.part_p[b];
-    for (int b = threadIdx.x; b < int(gridDim.x); b += kThreads) {
-        d += v.part_d[2 * b];
-        c += v.part_d[2 * b + 1];
-    }
-    double r3[3] = {p, d, c};
-    cta_sum<3>(r3, red);
-    if (threadIdx.x == 0) {
-        decide(v, r3[0], r3[1], r3[2]);
-        v.ctl->arrive = 0;
-    }
-}
-
-// ------------------------------------------------------------------ Halpern commit
-// commit_primal / commit_dual Halpern branches (src/cuda.cu:336-370), written in the
-// CPU backend's form (src/cpu.cpp:174-187): T = trial, old = current.
-__global__ void halpern_commit(int64_t n, int64_t m, Vecs v, bool fp32g) {
-    const Control &s = *v.ctl;
-    if (s.accept == 0)
-        return;
-    int cur = s.cur;
-    double lam = s.lambda, r = v.reflection;
-    double *x = cur ? v.x1 : v.x0;
-    const double *xt = cur ? v.x0 : v.x1;
-    double *y = cur ? v.y1 : v.y0;
-    const double *yt = cur ? v.y0 : v.y1;
-    double *ax = cur ? v.ax1 : v.ax0;
-    const double *axt = cur ? v.ax0 : v.ax1;
-    float *y32 = cur ? v.y32_1 : v.y32_0;
-    int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < n; j += stride) {
-        double T = xt[j], old = x[j];
-        v.xa[j] = T;
-        x[j] = lam * v.anchor_x[j] + (1 - lam) * ((1 + r) * T - r * old);
-    }
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += stride) {
-        double T = yt[i], old = y[i];
-        v.ya[i] = T;
-        double ny = lam * v.anchor_y[i] + (1 - lam) * ((1 + r) * T - r * old);
-        y[i] = ny;
-        if (fp32g)
-            y32[i] = float(ny);
-        ax[i] = lam * v.anchor_ax[i] + (1 - lam) * ((1 + r) * axt[i] - r * ax[i]);
-    }
-}
-
-// Fold a pending averaging step into xa / ya (commit of the last accepted trial).
-__global__ void flush_average(int64_t n, int64_t m, Vecs v) {
-    const Control &s = *v.ctl;
-    if (!s.pending)
-        return;
-    double w = s.pending_w;
-    const double *x = s.cur ? v.x1 : v.x0;
-    const double *y = s.cur ? v.y1 : v.y0;
-    int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < n; j += stride)
-        v.xa[j] = v.xa[j] + (x[j] - v.xa[j]) * w;
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += stride)
-        v.ya[i] = v.ya[i] + (y[i] - v.ya[i]) * w;
-}
-__global__ void clear_pending(Control *s) { s->pending = 0; }
-
-// ------------------------------------------------------------------ plain SpMV
-// out = M * x (with out_shift: out written through the current-buffer index when
-// `which` is non-null: out = which->cur ? out1 : out0).
-template <class Acc, class V, class P, class I, class X>
-__global__ void __launch_bounds__(kThreads) spmv_kernel(Csr<V, P, I> M, Schedule S, const X *x,
-                                                        double *out) {
-    sweep<Acc>(M, S, x, [&](int64_t r, Acc s, bool leader, bool, auto, int) {
-        if (leader)
-            out[r] = double(s);
-    });
-}
-
-// ------------------------------------------------------------------ monitor
-// Scaled-space KKT proxy of the reference's monitor_partial / monitor_reduce
-// (src/cuda.cu:387-446), one launch with a last-CTA reduction.
-__global__ void monitor_kernel(int64_t n, int64_t rows, const double *x, const double *y,
-                               const double *ax, const double *aty, const double *qx,
-                               const double *c, const double *q, const double *lb,
-                               const double *ub, const double *rl, const double *ru, double cscale,
-                               double *partial, unsigned *arrive, double *result) {
-    __shared__ double red[kWarps * 5];
-    __shared__ bool last;
-    double pr = 0, du = 0, ob = 0, co = 0, bd = 0;
-    int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    int64_t top = n > rows ? n : rows;
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < top; i += stride) {
-        if (i < n) {
-            double g = c[i] + q[i] * x[i] + aty[i] + (qx ? qx[i] : 0);
-            pr = fmax(pr, fmax(0., fmax(lb[i] - x[i], x[i] - ub[i])) / (1 + fabs(x[i])));
-            du = fmax(du, fabs(fmin(x[i] - lb[i], fmax(x[i] - ub[i], g))) / cscale);
-            double o = c[i] * x[i] + .5 * q[i] * x[i] * x[i] + (qx ? .5 * qx[i] * x[i] : 0);
-            ob += o;
-            if (g > 0 && isfinite(lb[i]))
-                co += fabs(g * (x[i] - lb[i]));
-            if (g < 0 && isfinite(ub[i]))
-                co += fabs(g * (ub[i] - x[i]));
-            if (!isfinite(x[i]) || !isfinite(g) || !isfinite(o))
-                bd = 1;
-        }
-        if (i < rows) {
-            if (isfinite(rl[i]))
-                pr = fmax(pr, fmax(0., rl[i] - ax[i]) / (1 + fabs(rl[i])));
-            if (isfinite(ru[i]))
-                pr = fmax(pr, fmax(0., ax[i] - ru[i]) / (1 + fabs(ru[i])));
-            if (y[i] != 0) {
-                double endpoint = y[i] > 0 ? ru[i] : rl[i];
-                if (isfinite(endpoint))
-                    co += fabs(y[i] * (endpoint - ax[i]));
-                else
-                    du = fmax(du, fabs(y[i]));
-            }
-            if (!isfinite(ax[i]) || !isfinite(y[i]))
-                bd = 1;
-        }
-    }
-    // max-reductions: transport as sums of per-warp maxima through a fixed tree
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        pr = fmax(pr, __shfl_xor_sync(0xffffffffu, pr, off));
-        du = fmax(du, __shfl_xor_sync(0xffffffffu, du, off));
-        bd = fmax(bd, __shfl_xor_sync(0xffffffffu, bd, off));
-        ob += __shfl_xor_sync(0xffffffffu, ob, off);
-        co += __shfl_xor_sync(0xffffffffu, co, off);
-    }
-    int w = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) {
-        red[w * 5 + 0] = pr;
-        red[w * 5 + 1] = du;
-        red[w * 5 + 2] = ob;
-        red[w * 5 + 3] = co;
-        red[w * 5 + 4] = bd;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double a[5] = {0, 0, 0, 0, 0};
-        for (int i = 0; i < kWarps; ++i) {
-            a[0] = fmax(a[0], red[i * 5 + 0]);
-            a[1] = fmax(a[1], red[i * 5 + 1]);
-            a[2] += red[i * 5 + 2];
-            a[3] += red[i * 5 + 3];
-            a[4] = fmax(a[4], red[i * 5 + 4]);
-        }
-        for (int t = 0; t < 5; ++t)
-            partial[5 * blockIdx.x + t] = a[t];
-        __threadfence();
-        last = atomicAdd(arrive, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!last || threadIdx.x != 0)
-        return;
-    __threadfence();
-    double a[5] = {0, 0, 0, 0, 0};
-    for (unsigned b = 0; b < gridDim.x; ++b) {
-        a[0] = fmax(a[0], partial[5 * b + 0]);
-        a[1] = fmax(a[1], partial[5 * b + 1]);
-        a[2] += partial[5 * b + 2];
-        a[3] += partial[5 * b + 3];
-        a[4] = fmax(a[4], partial[5 * b + 4]);
-    }
-    *result = a[4] ? INFINITY : fmax(fmax(a[0], a[1]), a[3] / (1 + fabs(a[2])));
-    *arrive = 0;
-}
-
-// ------------------------------------------------------------------ setup kernels
-__global__ void check_indices(int64_t nnz, const int64_t *idx, const double *val, int64_t cols,
-                              int *bad) {
-    int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < nnz; k += stride)
-        if (idx[k] < 0 || idx[k] >= cols || !isfinite(val[k]))
-            atomicOr(bad, 1);
-}
-template <class P> __global__ void narrow_ptr(int64_t n, const int64_t *src, P *dst) {
-    int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += stride)
-        dst[k] = P(src[k]);
-}
-template <class I, class V>
-__global__ void convert_entries(int64_t nnz, const int64_t *idx, const double *val, I *di, V *dv) {
-    int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < nnz; k += stride) {
-        di[k] = I(idx[k]);
-        dv[k] = V(val[k]);
-    }
-}
-__global__ void fp32_flags(int64_t nnz, const double *val, int *bad) {
-    int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < nnz; k += stride) {
-        float f = float(val[k]);
-        if (!isfinite(f) || (val[k] != 0 && f == 0))
-            atomicOr(bad, 1);
-    }
-}
-// Row id of every entry (for the transpose).
-__global__ void expand_rows(int64_t rows, const int64_t *ptr, int32_t *rowid) {
-    int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < rows; i += stride)
-        for (int64_t k = ptr[i]; k < ptr[i + 1]; ++k)
-            rowid[k] = int32_t(i);
-}
-__global__ void iota64(int64_t n, int64_t *a) {
-    int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += stride)
-        a[k] = k;
-}
-__global__ void count_cols(int64_t nnz, const int64_t *idx, int64_t *counts) {
-    int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < nnz; k += stride)
-        atomicAdd(reinterpret_cast<unsigned long long *>(counts + idx[k]), 1ull);
-}
-__global__ void gather_transpose(int64_t nnz, const int64_t *perm, const int32_t *rowid,
-                                 const double *val, int64_t *tidx, double *tval) {
-    int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < nnz; p += stride) {
-        int64_t k = perm[p];
-        tidx[p] = rowid[k];
-        tval[p] = val[k];
-    }
-}
-__global__ void to_float(int64_t n, const double *src, float *dst) {
-    int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += stride)
-        dst[k] = float(src[k]);
-}
-
-// ------------------------------------------------------------------ host side
 inline int grid_for(int64_t n, int cap = 148 * 8) {
     int64_t g = (n + kThreads - 1) / kThreads;
     return int(std::max<int64_t>(1, std::min<int64_t>(g, cap)));
 }
 
-// A device CSR in one of the engine's storage formats, with its row schedule.
-struct DeviceMatrix {
-    int64_t rows = 0, cols = 0, nnz = 0;
-    bool wide = false; // int64 ptr/idx
+// ------------------------------------------------------------------ matrices
+// A matrix in SELL-32 on the device (see nk_sell.cuh).
+struct SellMatrix {
+    int64_t rows = 0, cols = 0, nnz = 0, nv = 0, nsv = 0, nsr = 0, padded = 0;
+    bool wide = false; // int64 column indices
     int vbits = 64;    // 64 (double) or 32 (float) values
-    DevBuf<int32_t> ptr32, idx32;
-    DevBuf<int64_t> ptr64, idx64;
+    DevBuf<int64_t> cptr;
+    DevBuf<int32_t> len;
+    DevBuf<int32_t> idx32;
+    DevBuf<int64_t> idx64;
     DevBuf<double> val64;
     DevBuf<float> val32;
-    // schedule
-    DevBuf<int4> items;
-    DevBuf<int64_t> longrows;
-    int nitems = 0;
-    int64_t long_threshold = 0;
-    int width = 0; // sub-warp width of regular tiles
-    std::vector<int64_t> host_ptr;
+    DevBuf<int4> seg;
+    DevBuf<double> slots;
+    DevBuf<unsigned> counters;
 
-    template <class V, class P, class I> Csr<V, P, I> view() const {
-        Csr<V, P, I> c;
-        c.rows = rows;
-        if constexpr (sizeof(P) == 8)
-            c.ptr = reinterpret_cast<const P *>(ptr64.p);
-        else
-            c.ptr = reinterpret_cast<const P *>(ptr32.p);
+    template <class V, class I> Sell<V, I> view() const {
+        Sell<V, I> s;
+        s.cptr = cptr.p;
+        s.len = len.p;
         if constexpr (sizeof(I) == 8)
-            c.idx = reinterpret_cast<const I *>(idx64.p);
+            s.idx = reinterpret_cast<const I *>(idx64.p);
         else
-            c.idx = reinterpret_cast<const I *>(idx32.p);
+            s.idx = reinterpret_cast<const I *>(idx32.p);
         if constexpr (sizeof(V) == 8)
-            c.val = reinterpret_cast<const V *>(val64.p);
+            s.val = reinterpret_cast<const V *>(val64.p);
         else
-            c.val = reinterpret_cast<const V *>(val32.p);
-        return c;
+            s.val = reinterpret_cast<const V *>(val32.p);
+        s.nv = nv;
+        s.nsv = nsv;
+        s.nsr = nsr;
+        s.seg = seg.p;
+        s.slots = slots.p;
+        s.counters = counters.p;
+        return s;
     }
-    Schedule schedule() const { return Schedule{items.p, longrows.p, nitems, long_threshold}; }
     size_t device_bytes() const {
-        return ptr32.bytes() + idx32.bytes() + ptr64.bytes() + idx64.bytes() + val64.bytes() +
-               val32.bytes() + items.bytes() + longrows.bytes();
+        return cptr.bytes() + len.bytes() + idx32.bytes() + idx64.bytes() + val64.bytes() +
+               val32.bytes() + seg.bytes() + slots.bytes() + counters.bytes();
     }
 };
 
-// Row schedule: tiles of consecutive rows for a sub-warp width chosen from the
-// mean row length, long rows split out to warp-per-row and CTA-per-row items.
-void build_schedule(DeviceMatrix &M, int width_hint, int64_t threshold_hint) {
-    const auto &p = M.host_ptr;
-    int64_t R = M.rows;
-    int W = width_hint;
-    if (W <= 0) {
-        // width from the body of the length distribution (rows of at most 64
-        // entries); the tail goes to warp- and CTA-per-row items
-        int64_t body_rows = 0, body_nnz = 0;
-        for (int64_t r = 0; r < R; ++r) {
-            int64_t len = p[r + 1] - p[r];
-            if (len <= 64) {
-                ++body_rows;
-                body_nnz += len;
-            }
-        }
-        double mean = body_rows ? double(body_nnz) / double(body_rows) : 1;
-        W = 2;
-        while (W < 32 && W < mean)
-            W *= 2;
+// Sparse Q in CSR, engine order on both sides.
+struct QMatrix {
+    int64_t n = 0, nnz = 0;
+    bool wide = false;
+    int vbits = 64;
+    DevBuf<int64_t> ptr, idx64;
+    DevBuf<int32_t> idx32;
+    DevBuf<double> val64;
+    DevBuf<float> val32;
+    template <class V, class I> QCsr<V, I> view() const {
+        QCsr<V, I> q;
+        q.ptr = ptr.p;
+        if constexpr (sizeof(I) == 8)
+            q.idx = reinterpret_cast<const I *>(idx64.p);
+        else
+            q.idx = reinterpret_cast<const I *>(idx32.p);
+        if constexpr (sizeof(V) == 8)
+            q.val = reinterpret_cast<const V *>(val64.p);
+        else
+            q.val = reinterpret_cast<const V *>(val32.p);
+        return q;
     }
-    int64_t thr = threshold_hint > 0 ? threshold_hint : std::max<int64_t>(int64_t(4) * W, 32);
-    M.width = W;
-    M.long_threshold = thr;
-    std::vector<int4> items;
-    int per = kThreads / W;
-    for (int64_t r = 0; r < R; r += per) {
-        int cnt = int(std::min<int64_t>(per, R - r));
-        items.push_back(make_int4(W, int(r), cnt, 0));
+    size_t device_bytes() const {
+        return ptr.bytes() + idx64.bytes() + idx32.bytes() + val64.bytes() + val32.bytes();
     }
-    std::vector<int64_t> longs;
-    for (int64_t r = 0; r < R; ++r)
-        if (p[r + 1] - p[r] > thr)
-            longs.push_back(r);
-    std::stable_sort(longs.begin(), longs.end(),
-                     [&](int64_t a, int64_t b) { return p[a + 1] - p[a] > p[b + 1] - p[b]; });
-    const int64_t cta_threshold = 4096;
-    size_t k = 0;
-    for (; k < longs.size() && p[longs[k] + 1] - p[longs[k]] > cta_threshold; ++k)
-        items.push_back(make_int4(KIND_CTA, int(k), 1, 0));
-    for (; k < longs.size(); k += kWarps) {
-        int cnt = int(std::min<size_t>(kWarps, longs.size() - k));
-        items.push_back(make_int4(KIND_WARP, int(k), cnt, 0));
+};
+
+// Stable order of items by decreasing length (counting sort): result[k] is the
+// item placed k-th.
+std::vector<int64_t> order_by_length_desc(const std::vector<int64_t> &len) {
+    int64_t top = 0;
+    for (int64_t l : len)
+        top = std::max(top, l);
+    std::vector<int64_t> count(size_t(top + 2), 0);
+    for (int64_t l : len)
+        ++count[size_t(l)];
+    std::vector<int64_t> start(size_t(top + 2), 0); // first slot of each length, longest first
+    int64_t at = 0;
+    for (int64_t l = top; l >= 0; --l) {
+        start[size_t(l)] = at;
+        at += count[size_t(l)];
     }
-    // Put the heavy items first so the persistent grid starts on them.
-    std::stable_sort(items.begin(), items.end(), [](const int4 &a, const int4 &b) {
-        return (a.x > 32) > (b.x > 32);
-    });
-    M.nitems = int(items.size());
-    M.items.alloc(std::max<size_t>(1, items.size()));
-    if (!items.empty())
-        cuda_check(cudaMemcpy(M.items.p, items.data(), items.size() * sizeof(int4),
-                              cudaMemcpyHostToDevice),
-                   "schedule upload");
-    M.longrows.alloc(std::max<size_t>(1, longs.size()));
-    if (!longs.empty())
-        cuda_check(cudaMemcpy(M.longrows.p, longs.data(), longs.size() * sizeof(int64_t),
-                              cudaMemcpyHostToDevice),
-                   "long rows upload");
+    std::vector<int64_t> order(len.size());
+    for (size_t i = 0; i < len.size(); ++i)
+        order[size_t(start[size_t(len[i])]++)] = int64_t(i);
+    return order;
 }
 
-// Upload a host CSR (int64 ptr/index, double values) into the engine format.
-// `dptr/didx/dval` may already hold the int64/double arrays on the device.
-void fill_matrix(DeviceMatrix &M, int64_t rows, int64_t cols, const int64_t *dptr,
-                 const int64_t *didx, const double *dval, bool wide, int vbits,
-                 cudaStream_t stream) {
+struct SellPlan {
+    std::vector<int64_t> cptr, src;
+    std::vector<int32_t> len;
+    std::vector<int4> seg;
+    int64_t nv = 0, nsv = 0, nsr = 0;
+};
+
+// Virtual rows and chunks for an engine-order CSR (rows sorted longest first):
+// rows longer than `split` become consecutive segments of at most `split`
+// entries, placed first; chunks of 32 virtual rows are padded to their longest.
+SellPlan plan_sell(const std::vector<int64_t> &ptr, int64_t rows, int64_t split) {
+    SellPlan P;
+    while (P.nsr < rows && ptr[size_t(P.nsr + 1)] - ptr[size_t(P.nsr)] > split)
+        ++P.nsr;
+    for (int64_t r = 0; r < P.nsr; ++r) {
+        int64_t L = ptr[size_t(r + 1)] - ptr[size_t(r)];
+        int nseg = int((L + split - 1) / split);
+        int first = int(P.len.size());
+        for (int s = 0; s < nseg; ++s) {
+            P.len.push_back(int32_t(std::min<int64_t>(split, L - int64_t(s) * split)));
+            P.src.push_back(ptr[size_t(r)] + int64_t(s) * split);
+            P.seg.push_back(make_int4(int(r), first, nseg, int(r)));
+        }
+    }
+    P.nsv = int64_t(P.len.size());
+    for (int64_t r = P.nsr; r < rows; ++r) {
+        P.len.push_back(int32_t(ptr[size_t(r + 1)] - ptr[size_t(r)]));
+        P.src.push_back(ptr[size_t(r)]);
+    }
+    P.nv = int64_t(P.len.size());
+    int64_t nchunks = (P.nv + 31) / 32;
+    P.cptr.assign(size_t(nchunks + 1), 0);
+    for (int64_t c = 0; c < nchunks; ++c) {
+        int32_t top = 0;
+        for (int64_t v = 32 * c; v < std::min(P.nv, 32 * c + 32); ++v)
+            top = std::max(top, P.len[size_t(v)]);
+        P.cptr[size_t(c + 1)] = P.cptr[size_t(c)] + 32 * int64_t(top);
+    }
+    return P;
+}
+
+template <class T> void upload_vector(DevBuf<T> &d, const std::vector<T> &h, cudaStream_t s) {
+    d.alloc(std::max<size_t>(1, h.size()));
+    if (!h.empty())
+        cuda_check(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s),
+                   "upload");
+}
+
+// SELL-32 from an engine-order CSR (host ptr, device int64 indices / double values).
+void build_sell(SellMatrix &M, int64_t rows, int64_t cols, const std::vector<int64_t> &ptr,
+                const int64_t *cidx, const double *cval, bool wide, int vbits, cudaStream_t s) {
     M.rows = rows;
     M.cols = cols;
+    M.nnz = ptr[size_t(rows)];
     M.wide = wide;
     M.vbits = vbits;
-    M.host_ptr.resize(size_t(rows + 1));
-    cuda_check(cudaMemcpyAsync(M.host_ptr.data(), dptr, size_t(rows + 1) * sizeof(int64_t),
-                               cudaMemcpyDeviceToHost, stream),
-               "ptr download");
-    cuda_check(cudaStreamSynchronize(stream), "ptr download");
-    M.nnz = M.host_ptr[size_t(rows)];
-    int g = grid_for(std::max<int64_t>(M.nnz, rows + 1), 148 * 32);
+    SellPlan P = plan_sell(ptr, rows, NK_SPLIT);
+    M.nv = P.nv;
+    M.nsv = P.nsv;
+    M.nsr = P.nsr;
+    M.padded = P.cptr.back();
+    upload_vector(M.cptr, P.cptr, s);
+    upload_vector(M.len, P.len, s);
+    upload_vector(M.seg, P.seg, s);
+    DevBuf<int64_t> src;
+    upload_vector(src, P.src, s);
+    M.slots.alloc(size_t(std::max<int64_t>(1, P.nsv)));
+    M.counters.alloc(size_t(std::max<int64_t>(1, P.nsr)));
+    cuda_check(cudaMemsetAsync(M.counters.p, 0, M.counters.bytes(), s), "split counters");
+    size_t total = size_t(std::max<int64_t>(1, M.padded));
     if (wide) {
-        M.ptr64.alloc(size_t(rows + 1));
-        M.idx64.alloc(std::max<int64_t>(1, M.nnz));
-        cuda_check(cudaMemcpyAsync(M.ptr64.p, dptr, size_t(rows + 1) * 8, cudaMemcpyDeviceToDevice,
-                                   stream),
-                   "ptr copy");
+        M.idx64.alloc(total);
+        cuda_check(cudaMemsetAsync(M.idx64.p, 0, M.idx64.bytes(), s), "sell idx");
     } else {
-        M.ptr32.alloc(size_t(rows + 1));
-        M.idx32.alloc(std::max<int64_t>(1, M.nnz));
-        narrow_ptr<int32_t><<<g, kThreads, 0, stream>>>(rows + 1, dptr, M.ptr32.p);
+        M.idx32.alloc(total);
+        cuda_check(cudaMemsetAsync(M.idx32.p, 0, M.idx32.bytes(), s), "sell idx");
     }
-    if (vbits == 64)
-        M.val64.alloc(std::max<int64_t>(1, M.nnz));
-    else
-        M.val32.alloc(std::max<int64_t>(1, M.nnz));
-    if (M.nnz) {
+    if (vbits == 64) {
+        M.val64.alloc(total);
+        cuda_check(cudaMemsetAsync(M.val64.p, 0, M.val64.bytes(), s), "sell val");
+    } else {
+        M.val32.alloc(total);
+        cuda_check(cudaMemsetAsync(M.val32.p, 0, M.val32.bytes(), s), "sell val");
+    }
+    if (M.nv) {
+        int g = grid_for(M.nv, 148 * 32);
         if (wide && vbits == 64)
-            convert_entries<int64_t, double><<<g, kThreads, 0, stream>>>(M.nnz, didx, dval,
-                                                                        M.idx64.p, M.val64.p);
+            fill_sell<double, int64_t><<<g, kThreads, 0, s>>>(M.nv, src.p, M.len.p, M.cptr.p, cidx,
+                                                               cval, M.idx64.p, M.val64.p);
         else if (wide)
-            convert_entries<int64_t, float><<<g, kThreads, 0, stream>>>(M.nnz, didx, dval,
-                                                                       M.idx64.p, M.val32.p);
+            fill_sell<float, int64_t><<<g, kThreads, 0, s>>>(M.nv, src.p, M.len.p, M.cptr.p, cidx,
+                                                              cval, M.idx64.p, M.val32.p);
         else if (vbits == 64)
-            convert_entries<int32_t, double><<<g, kThreads, 0, stream>>>(M.nnz, didx, dval,
-                                                                        M.idx32.p, M.val64.p);
+            fill_sell<double, int32_t><<<g, kThreads, 0, s>>>(M.nv, src.p, M.len.p, M.cptr.p, cidx,
+                                                               cval, M.idx32.p, M.val64.p);
         else
-            convert_entries<int32_t, float><<<g, kThreads, 0, stream>>>(M.nnz, didx, dval,
-                                                                       M.idx32.p, M.val32.p);
+            fill_sell<float, int32_t><<<g, kThreads, 0, s>>>(M.nv, src.p, M.len.p, M.cptr.p, cidx,
+                                                              cval, M.idx32.p, M.val32.p);
+        cuda_check(cudaGetLastError(), "sell fill");
     }
-    cuda_check(cudaGetLastError(), "matrix conversion");
+    cuda_check(cudaStreamSynchronize(s), "sell build");
 }
 
+// Build the explicit transpose on the device: a stable radix sort of the column
+// indices carries every entry to its row of A^T in increasing row order, the
+// order Sparse::transpose produces (src/model.cpp:39-58).
+void device_transpose(int64_t rows, int64_t cols, int64_t nnz, const int64_t *dptr,
+                      const int64_t *didx, const double *dval, DevBuf<int64_t> &tptr,
+                      DevBuf<int64_t> &tidx, DevBuf<double> &tval, cudaStream_t stream) {
+    tptr.alloc(size_t(cols + 1));
+    tidx.alloc(std::max<int64_t>(1, nnz));
+    tval.alloc(std::max<int64_t>(1, nnz));
+    DevBuf<int64_t> counts(static_cast<size_t>(cols + 1));
+    cuda_check(cudaMemsetAsync(counts.p, 0, size_t(cols + 1) * 8, stream), "counts");
+    if (nnz) {
+        int g = grid_for(nnz, 148 * 32);
+        count_cols<<<g, kThreads, 0, stream>>>(nnz, didx, counts.p);
+        DevBuf<int32_t> rowid(static_cast<size_t>(nnz));
+        expand_rows<<<grid_for(rows, 148 * 32), kThreads, 0, stream>>>(rows, dptr, rowid.p);
+        DevBuf<int64_t> keys_out(static_cast<size_t>(nnz)), perm_in(static_cast<size_t>(nnz)),
+            perm_out(static_cast<size_t>(nnz));
+        iota64<<<g, kThreads, 0, stream>>>(nnz, perm_in.p);
+        int end_bit = 1;
+        while (end_bit < 63 && (int64_t(1) << end_bit) < cols)
+            ++end_bit;
+        size_t temp = 0;
+        cuda_check(cub::DeviceRadixSort::SortPairs(nullptr, temp, didx, keys_out.p, perm_in.p,
+                                                   perm_out.p, nnz, 0, end_bit, stream),
+                   "transpose sort size");
+        DevBuf<char> work(temp);
+        cuda_check(cub::DeviceRadixSort::SortPairs(work.p, temp, didx, keys_out.p, perm_in.p,
+                                                   perm_out.p, nnz, 0, end_bit, stream),
+                   "transpose sort");
+        gather_transpose<<<g, kThreads, 0, stream>>>(nnz, perm_out.p, rowid.p, dval, tidx.p,
+                                                    tval.p);
+        cuda_check(cudaGetLastError(), "transpose gather");
+        size_t t2 = 0;
+        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, t2, counts.p, tptr.p, cols + 1, stream),
+                   "transpose scan size");
+        DevBuf<char> w2(t2);
+        cuda_check(cub::DeviceScan::ExclusiveSum(w2.p, t2, counts.p, tptr.p, cols + 1, stream),
+                   "transpose scan");
+        cuda_check(cudaStreamSynchronize(stream), "transpose");
+    } else {
+        cuda_check(cudaMemsetAsync(tptr.p, 0, size_t(cols + 1) * 8, stream), "empty transpose");
+        cuda_check(cudaStreamSynchronize(stream), "transpose");
+    }
+}
+
+// Engine-order CSR of a device CSR: rows in `perm` order, column indices through
+// `inv`.  Returns the new host ptr; the device arrays land in (idx, val).
+std::vector<int64_t> permute_device_csr(int64_t rows, const std::vector<int64_t> &src_ptr_h,
+                                        const int64_t *src_ptr, const int64_t *src_idx,
+                                        const double *src_val, const std::vector<int64_t> &perm,
+                                        const int64_t *dperm, const int64_t *dinv,
+                                        DevBuf<int64_t> &idx, DevBuf<double> &val,
+                                        cudaStream_t s) {
+    std::vector<int64_t> ptr(static_cast<size_t>(rows + 1), 0);
+    for (int64_t i = 0; i < rows; ++i) {
+        int64_t o = perm[size_t(i)];
+        ptr[size_t(i + 1)] = ptr[size_t(i)] + (src_ptr_h[size_t(o + 1)] - src_ptr_h[size_t(o)]);
+    }
+    int64_t nnz = ptr[size_t(rows)];
+    DevBuf<int64_t> dptr;
+    upload_vector(dptr, ptr, s);
+    idx.alloc(std::max<int64_t>(1, nnz));
+    val.alloc(std::max<int64_t>(1, nnz));
+    if (rows && nnz) {
+        permute_csr<<<grid_for(rows * 32, 148 * 32), kThreads, 0, s>>>(
+            rows, dperm, dinv, src_ptr, src_idx, src_val, dptr.p, idx.p, val.p);
+        cuda_check(cudaGetLastError(), "csr permutation");
+    }
+    cuda_check(cudaStreamSynchronize(s), "csr permutation");
+    return ptr;
+}
+
+void validate_csr(const nk_csr *M, int64_t rows, int64_t cols, const char *what) {
+    if (!M || M->rows != rows || M->cols != cols || !M->ptr)
+        throw Error(NK_ERR_INVALID, std::string("inconsistent ") + what + " dimensions");
+    if (M->ptr[0] != 0)
+        throw Error(NK_ERR_INVALID, std::string("invalid ") + what + " CSR storage");
+    for (int64_t i = 0; i < rows; ++i)
+        if (M->ptr[i + 1] < M->ptr[i])
+            throw Error(NK_ERR_INVALID, std::string("invalid ") + what + " CSR offsets");
+    if (M->ptr[rows] > 0 && (!M->index || !M->value))
+        throw Error(NK_ERR_INVALID, std::string("missing ") + what + " entries");
+}
+
+// Upload a host CSR as int64/double device arrays and check its indices (and,
+// for FP32 storage, that every coefficient survives the conversion).
+void upload_raw(const nk_csr *H, int vbits, cudaStream_t stream, DevBuf<int64_t> &p,
+                DevBuf<int64_t> &ix, DevBuf<double> &vv) {
+    int64_t nnz = H->ptr[H->rows];
+    p.alloc(static_cast<size_t>(H->rows + 1));
+    ix.alloc(std::max<int64_t>(1, nnz));
+    vv.alloc(std::max<int64_t>(1, nnz));
+    cuda_check(cudaMemcpyAsync(p.p, H->ptr, size_t(H->rows + 1) * 8, cudaMemcpyHostToDevice, stream),
+               "ptr upload");
+    if (nnz) {
+        cuda_check(cudaMemcpyAsync(ix.p, H->index, size_t(nnz) * 8, cudaMemcpyHostToDevice, stream),
+                   "index upload");
+        cuda_check(cudaMemcpyAsync(vv.p, H->value, size_t(nnz) * 8, cudaMemcpyHostToDevice, stream),
+                   "value upload");
+        DevBuf<int> bad(1);
+        cuda_check(cudaMemsetAsync(bad.p, 0, sizeof(int), stream), "flag");
+        check_indices<<<grid_for(nnz, 148 * 32), kThreads, 0, stream>>>(nnz, ix.p, vv.p, H->cols,
+                                                                        bad.p);
+        if (vbits == 32)
+            fp32_flags<<<grid_for(nnz, 148 * 32), kThreads, 0, stream>>>(nnz, vv.p, bad.p);
+        int hb = 0;
+        cuda_check(cudaMemcpyAsync(&hb, bad.p, sizeof(int), cudaMemcpyDeviceToHost, stream), "flag");
+        cuda_check(cudaStreamSynchronize(stream), "index check");
+        if (hb)
+            throw Error(NK_ERR_INVALID,
+                        vbits == 32 ? "invalid coefficient/index, or FP32 matrix conversion would "
+                                      "overflow or erase a coefficient; use fp64"
+                                    : "Invalid matrix coefficient/index");
+    }
+    cuda_check(cudaStreamSynchronize(stream), "matrix upload");
+}
+
+// ------------------------------------------------------------------ engine
 struct Engine {
     int64_t n = 0, m = 0;
     bool adaptive = false, halpern = false, residual_restarts = false, graphs = false;
@@ -636,20 +352,27 @@ struct Engine {
     int precision = NK_PRECISION_FP64;
     double reflection = 0, a_norm = 0, q_norm = 0;
     cudaStream_t stream = nullptr;
-    DeviceMatrix A, At, Q;
+    SellMatrix A, At;
+    QMatrix Q;
     DevBuf<double> c, q, lb, ub, rl, ru, x[2], y[2], ax[2], xa, ya, dx, anchor_x, anchor_y,
         anchor_ax, part_p, part_d, mon_ax, mon_aty, mon_qx, mon_part, mon_out;
     DevBuf<float> dx32, y32[2];
     DevBuf<Control> ctl;
     DevBuf<unsigned> mon_arrive;
     Control *host_ctl = nullptr; // pinned mirror
-    int grid_p = 1, grid_d = 1;
+    int grid_p = 1, grid_d = 1, grid_s = 148;
     int64_t accepted = 0, rejected = 0, trials = 0;
     int empty_chunks = 0;
     bool request_restart = false;
-    double graph_tau = NAN, graph_sigma = NAN;
     cudaGraphExec_t graph_exec[8] = {};
     double cscale = 1;
+    // engine order: engine column j is the caller's column col_perm[j], engine
+    // row i the caller's row row_perm[i]
+    DevBuf<int64_t> col_perm, row_perm;
+    DevBuf<double> scratch_n, scratch_m;
+    // per-kernel timing hooks: when set, events are recorded around the primal
+    // and dual launches of each trial (profiling mode, no graphs)
+    cudaEvent_t ev[4] = {};
 
     ~Engine() {
         if (stream)
@@ -695,81 +418,81 @@ struct Engine {
     }
 
     // -------------------------------------------------------------- launches
-    template <class V, class P, class I> void launch_trial_t() {
+    template <class Acc, class V, class I> void launch_trial_t() {
         Vecs v = vecs();
-        auto at = At.view<V, P, I>();
-        auto a = A.view<V, P, I>();
-        auto qm = sparse_q ? Q.view<V, P, I>() : Csr<V, P, I>{nullptr, nullptr, nullptr, 0};
-        Schedule qs = sparse_q ? Q.schedule() : Schedule{};
+        constexpr bool F32 = sizeof(Acc) == 4;
+        auto at = At.view<V, I>();
+        auto a = A.view<V, I>();
+        auto qm = Q.view<V, I>();
         if (ev[0])
             cudaEventRecord(ev[0], stream);
-        if (precision == NK_PRECISION_FP32) {
-            if (sparse_q)
-                primal_kernel<float, V, P, I, true, true>
-                    <<<grid_p, kThreads, 0, stream>>>(at, At.schedule(), qm, qs, v);
-            else
-                primal_kernel<float, V, P, I, false, true>
-                    <<<grid_p, kThreads, 0, stream>>>(at, At.schedule(), qm, qs, v);
-            if (ev[1])
-                cudaEventRecord(ev[1], stream);
-            dual_kernel<float, V, P, I, true><<<grid_d, kThreads, 0, stream>>>(a, A.schedule(), v);
-        } else {
-            if (sparse_q)
-                primal_kernel<double, V, P, I, true, false>
-                    <<<grid_p, kThreads, 0, stream>>>(at, At.schedule(), qm, qs, v);
-            else
-                primal_kernel<double, V, P, I, false, false>
-                    <<<grid_p, kThreads, 0, stream>>>(at, At.schedule(), qm, qs, v);
-            if (ev[1])
-                cudaEventRecord(ev[1], stream);
-            dual_kernel<double, V, P, I, false><<<grid_d, kThreads, 0, stream>>>(a, A.schedule(), v);
-        }
+        if (sparse_q)
+            primal_kernel<Acc, V, I, true, F32><<<grid_p, kThreads, 0, stream>>>(at, qm, v);
+        else
+            primal_kernel<Acc, V, I, false, F32><<<grid_p, kThreads, 0, stream>>>(at, qm, v);
+        if (ev[1])
+            cudaEventRecord(ev[1], stream);
+        dual_kernel<Acc, V, I, F32><<<grid_d, kThreads, 0, stream>>>(a, v);
         if (ev[2])
             cudaEventRecord(ev[2], stream);
         if (halpern)
-            halpern_commit<<<grid_for(std::max(n, m)), kThreads, 0, stream>>>(
-                n, m, v, precision == NK_PRECISION_FP32);
+            halpern_commit<<<grid_for(std::max(n, m)), kThreads, 0, stream>>>(n, m, v, F32);
     }
-    // Per-kernel timing hooks: when non-null, events are recorded around the
-    // primal and dual launches of each trial (profiling mode, no graphs).
-    cudaEvent_t ev[4] = {};
     void launch_trial() {
         if (precision == NK_PRECISION_FP64) {
             if (wide)
-                launch_trial_t<double, int64_t, int64_t>();
+                launch_trial_t<double, double, int64_t>();
             else
-                launch_trial_t<double, int32_t, int32_t>();
+                launch_trial_t<double, double, int32_t>();
+        } else if (precision == NK_PRECISION_MIXED) {
+            if (wide)
+                launch_trial_t<double, float, int64_t>();
+            else
+                launch_trial_t<double, float, int32_t>();
         } else {
             if (wide)
-                launch_trial_t<float, int64_t, int64_t>();
+                launch_trial_t<float, float, int64_t>();
             else
-                launch_trial_t<float, int32_t, int32_t>();
+                launch_trial_t<float, float, int32_t>();
         }
     }
 
-    template <class V, class P, class I>
-    void spmv_t(const DeviceMatrix &M, const double *xin, double *out) {
-        if (M.rows == 0)
+    template <class V, class I>
+    void spmv_t(const SellMatrix &M, const double *xin, double *out) {
+        if (M.nv == 0)
             return;
-        int g = std::max(1, std::min(M.nitems, 148 * 8));
-        spmv_kernel<double, V, P, I, double>
-            <<<g, kThreads, 0, stream>>>(M.view<V, P, I>(), M.schedule(), xin, out);
+        int g = int(std::max<int64_t>(1, std::min<int64_t>((M.nv / 32 + kWarps) / kWarps, grid_s)));
+        spmv_kernel<V, I><<<g, kThreads, 0, stream>>>(M.view<V, I>(), xin, out);
     }
-    // out = M * xin with the FP64 accumulation path (used for activity rebasing,
-    // the monitor and tests).
-    void spmv(const DeviceMatrix &M, const double *xin, double *out) {
+    // out = M * xin with FP64 accumulation (activity rebasing, the monitor).
+    void spmv(const SellMatrix &M, const double *xin, double *out) {
         if (M.vbits == 64) {
             if (M.wide)
-                spmv_t<double, int64_t, int64_t>(M, xin, out);
+                spmv_t<double, int64_t>(M, xin, out);
             else
-                spmv_t<double, int32_t, int32_t>(M, xin, out);
+                spmv_t<double, int32_t>(M, xin, out);
         } else {
             if (M.wide)
-                spmv_t<float, int64_t, int64_t>(M, xin, out);
+                spmv_t<float, int64_t>(M, xin, out);
             else
-                spmv_t<float, int32_t, int32_t>(M, xin, out);
+                spmv_t<float, int32_t>(M, xin, out);
         }
         cuda_check(cudaGetLastError(), "spmv launch");
+    }
+    void q_spmv(const double *xin, double *out) {
+        int g = grid_for(n);
+        if (Q.vbits == 64) {
+            if (Q.wide)
+                q_spmv_kernel<double, int64_t><<<g, kThreads, 0, stream>>>(n, Q.view<double, int64_t>(), xin, out);
+            else
+                q_spmv_kernel<double, int32_t><<<g, kThreads, 0, stream>>>(n, Q.view<double, int32_t>(), xin, out);
+        } else {
+            if (Q.wide)
+                q_spmv_kernel<float, int64_t><<<g, kThreads, 0, stream>>>(n, Q.view<float, int64_t>(), xin, out);
+            else
+                q_spmv_kernel<float, int32_t><<<g, kThreads, 0, stream>>>(n, Q.view<float, int32_t>(), xin, out);
+        }
+        cuda_check(cudaGetLastError(), "Q spmv launch");
     }
 
     void sync_ctl() {
@@ -799,14 +522,8 @@ struct Engine {
             to_float<<<grid_for(m), kThreads, 0, stream>>>(m, y[cur].p, y32[cur].p);
     }
 
-    void clear_graphs() {
-        for (auto &g : graph_exec)
-            if (g) {
-                cudaGraphExecDestroy(g);
-                g = nullptr;
-            }
-    }
-    // Graph k holds 2^k trials.
+    // Graph k holds 2^k trials; kernels read tau, sigma and the iterate index
+    // from device memory, so graphs never need recapturing.
     cudaGraphExec_t graph_for(int k) {
         if (!graph_exec[k]) {
             cudaGraph_t g = nullptr;
@@ -875,22 +592,45 @@ struct Engine {
     void download(double *dst, const double *src, int64_t count) {
         if (count && dst)
             cuda_check(cudaMemcpyAsync(dst, src, size_t(count) * 8, cudaMemcpyDeviceToHost, stream),
-                       "candidate download");
+                       "download");
     }
     void upload(double *dst, const double *src, int64_t count) {
         if (count)
             cuda_check(cudaMemcpyAsync(dst, src, size_t(count) * 8, cudaMemcpyHostToDevice, stream),
                        "upload");
     }
+    // Vector transfers in the caller's order (columns: col_perm, rows: row_perm).
+    void download_perm(double *host, const double *dev, int64_t len, const DevBuf<int64_t> &perm,
+                       DevBuf<double> &scratch) {
+        if (!len || !host)
+            return;
+        scatter_vec<<<grid_for(len), kThreads, 0, stream>>>(len, perm.p, dev, scratch.p);
+        cuda_check(cudaGetLastError(), "scatter");
+        download(host, scratch.p, len);
+        cuda_check(cudaStreamSynchronize(stream), "download");
+    }
+    void upload_perm(double *dev, const double *host, int64_t len, const DevBuf<int64_t> &perm,
+                     DevBuf<double> &scratch) {
+        if (!len)
+            return;
+        upload(scratch.p, host, len);
+        gather_vec<<<grid_for(len), kThreads, 0, stream>>>(len, perm.p, scratch.p, dev);
+        cuda_check(cudaGetLastError(), "gather");
+        cuda_check(cudaStreamSynchronize(stream), "upload");
+    }
+    void download_x(double *h, const double *d) { download_perm(h, d, n, col_perm, scratch_n); }
+    void download_y(double *h, const double *d) { download_perm(h, d, m, row_perm, scratch_m); }
+    void upload_x(double *d, const double *h) { upload_perm(d, h, n, col_perm, scratch_n); }
+    void upload_y(double *d, const double *h) { upload_perm(d, h, m, row_perm, scratch_m); }
 
     void candidates(double *hx, double *hy, double *hxa, double *hya) {
         flush();
         sync_ctl();
         int cur = host_ctl->cur;
-        download(hx, x[cur].p, n);
-        download(hy, y[cur].p, m);
-        download(hxa, xa.p, n);
-        download(hya, ya.p, m);
+        download_x(hx, x[cur].p);
+        download_y(hy, y[cur].p);
+        download_x(hxa, xa.p);
+        download_y(hya, ya.p);
         refresh_activity(cur); // rebase A*x like the reference (src/cuda.cu:874-891)
         cuda_check(cudaStreamSynchronize(stream), "candidates");
     }
@@ -952,8 +692,8 @@ struct Engine {
     void reset(const double *hx, const double *hy) {
         sync_ctl();
         int cur = host_ctl->cur;
-        upload(x[cur].p, hx, n);
-        upload(y[cur].p, hy, m);
+        upload_x(x[cur].p, hx);
+        upload_y(y[cur].p, hy);
         refresh_y32(cur);
         refresh_activity(cur);
         restart_state(cur);
@@ -982,16 +722,12 @@ struct Engine {
         for (int which = 0; which < 2; ++which) {
             const double *px = which ? xa.p : x[cur].p;
             const double *py = which ? ya.p : y[cur].p;
-            if (m && A.nnz)
+            if (m)
                 spmv(A, px, mon_ax.p);
-            else if (m)
-                cuda_check(cudaMemsetAsync(mon_ax.p, 0, size_t(m) * 8, stream), "monitor ax");
-            if (n && At.nnz)
+            if (n)
                 spmv(At, py, mon_aty.p);
-            else if (n)
-                cuda_check(cudaMemsetAsync(mon_aty.p, 0, size_t(n) * 8, stream), "monitor aty");
             if (sparse_q)
-                spmv(Q, px, mon_qx.p);
+                q_spmv(px, mon_qx.p);
             if (std::max(n, m) == 0)
                 return 0;
             int g = grid_for(std::max(n, m));
@@ -1009,11 +745,13 @@ struct Engine {
     }
 
     // snapshot parts: x, y, xa, ya, ax, anchor_x, anchor_y, anchor_ax, control(11),
-    // counters {accepted, rejected, empty_chunks, request_restart}
+    // counters {accepted, rejected, empty_chunks, request_restart}; vectors in
+    // the caller's order
     std::vector<int64_t> layout() const {
         int64_t hn = halpern ? n : 0, hm = halpern ? m : 0;
         return {n, m, n, m, m, hn, hm, hm, 11, 4};
     }
+    static bool column_part(int i) { return i == 0 || i == 2 || i == 5; }
     void snapshot(double *out) {
         flush();
         sync_ctl();
@@ -1023,7 +761,12 @@ struct Engine {
         const double *src[8] = {x[cur].p, y[cur].p, xa.p, ya.p, ax[cur].p,
                                 anchor_x.p, anchor_y.p, anchor_ax.p};
         for (int i = 0; i < 8; ++i) {
-            download(out + at, src[i], L[size_t(i)]);
+            if (L[size_t(i)]) {
+                if (column_part(i))
+                    download_x(out + at, src[i]);
+                else
+                    download_y(out + at, src[i]);
+            }
             at += L[size_t(i)];
         }
         cuda_check(cudaStreamSynchronize(stream), "snapshot");
@@ -1059,7 +802,12 @@ struct Engine {
                           anchor_x.p, anchor_y.p, anchor_ax.p};
         at = 0;
         for (int i = 0; i < 8; ++i) {
-            upload(dst[i], in + at, L[size_t(i)]);
+            if (L[size_t(i)]) {
+                if (column_part(i))
+                    upload_x(dst[i], in + at);
+                else
+                    upload_y(dst[i], in + at);
+            }
             at += L[size_t(i)];
         }
         refresh_y32(cur);
@@ -1129,115 +877,34 @@ struct Engine {
     size_t device_bytes() const {
         size_t b = A.device_bytes() + At.device_bytes() + Q.device_bytes();
         for (auto *d : {&c, &q, &lb, &ub, &rl, &ru, &x[0], &x[1], &y[0], &y[1], &ax[0], &ax[1],
-                        &xa, &ya, &dx, &anchor_x, &anchor_y, &anchor_ax, &part_p, &part_d})
+                        &xa, &ya, &dx, &anchor_x, &anchor_y, &anchor_ax, &part_p, &part_d,
+                        &scratch_n, &scratch_m})
             b += d->bytes();
-        b += dx32.bytes() + y32[0].bytes() + y32[1].bytes();
+        b += dx32.bytes() + y32[0].bytes() + y32[1].bytes() + col_perm.bytes() + row_perm.bytes();
         return b;
     }
 };
 
-// Build the explicit transpose on the device: stable radix sort of the column
-// indices carries every entry to its row of A^T in increasing row order, the
-// order Sparse::transpose produces (src/model.cpp:39-58).
-void device_transpose(int64_t rows, int64_t cols, int64_t nnz, const int64_t *dptr,
-                      const int64_t *didx, const double *dval, DevBuf<int64_t> &tptr,
-                      DevBuf<int64_t> &tidx, DevBuf<double> &tval, cudaStream_t stream) {
-    tptr.alloc(size_t(cols + 1));
-    tidx.alloc(std::max<int64_t>(1, nnz));
-    tval.alloc(std::max<int64_t>(1, nnz));
-    DevBuf<int64_t> counts(static_cast<size_t>(cols + 1));
-    cuda_check(cudaMemsetAsync(counts.p, 0, size_t(cols + 1) * 8, stream), "counts");
-    if (nnz) {
-        int g = grid_for(nnz, 148 * 32);
-        count_cols<<<g, kThreads, 0, stream>>>(nnz, didx, counts.p);
-        DevBuf<int32_t> rowid(static_cast<size_t>(nnz));
-        expand_rows<<<grid_for(rows, 148 * 32), kThreads, 0, stream>>>(rows, dptr, rowid.p);
-        DevBuf<int64_t> keys_out(static_cast<size_t>(nnz)), perm_in(static_cast<size_t>(nnz)),
-            perm_out(static_cast<size_t>(nnz));
-        iota64<<<g, kThreads, 0, stream>>>(nnz, perm_in.p);
-        int end_bit = 1;
-        while (end_bit < 63 && (int64_t(1) << end_bit) < cols)
-            ++end_bit;
-        size_t temp = 0;
-        cuda_check(cub::DeviceRadixSort::SortPairs(nullptr, temp, didx, keys_out.p, perm_in.p,
-                                                   perm_out.p, nnz, 0, end_bit, stream),
-                   "transpose sort size");
-        DevBuf<char> work(temp);
-        cuda_check(cub::DeviceRadixSort::SortPairs(work.p, temp, didx, keys_out.p, perm_in.p,
-                                                   perm_out.p, nnz, 0, end_bit, stream),
-                   "transpose sort");
-        gather_transpose<<<g, kThreads, 0, stream>>>(nnz, perm_out.p, rowid.p, dval, tidx.p,
-                                                    tval.p);
-        cuda_check(cudaGetLastError(), "transpose gather");
-        size_t t2 = 0;
-        cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, t2, counts.p, tptr.p, cols + 1, stream),
-                   "transpose scan size");
-        DevBuf<char> w2(t2);
-        cuda_check(cub::DeviceScan::ExclusiveSum(w2.p, t2, counts.p, tptr.p, cols + 1, stream),
-                   "transpose scan");
-        cuda_check(cudaStreamSynchronize(stream), "transpose");
-    } else {
-        cuda_check(cudaMemsetAsync(tptr.p, 0, size_t(cols + 1) * 8, stream), "empty transpose");
-    }
-}
-
-int occupancy_grid(const void *kernel, int nitems) {
-    int dev = 0, sms = 148, per = 4;
+// Persistent grid: as many CTAs as fit on the device at once, at most one warp
+// per SELL chunk.
+int occupancy_grid(const void *kernel, int64_t chunks) {
+    int dev = 0, sms = 148, per = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kThreads, 0);
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kThreads, 0),
+               "occupancy");
     per = std::max(1, per);
-    return std::max(1, std::min(nitems, sms * per));
+    int64_t need = (chunks + kWarps - 1) / kWarps;
+    return int(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sms) * per)));
 }
 
-void validate_csr(const nk_csr *M, int64_t rows, int64_t cols, const char *what) {
-    if (!M || M->rows != rows || M->cols != cols || !M->ptr)
-        throw Error(NK_ERR_INVALID, std::string("inconsistent ") + what + " dimensions");
-    if (M->ptr[0] != 0)
-        throw Error(NK_ERR_INVALID, std::string("invalid ") + what + " CSR storage");
-    for (int64_t i = 0; i < rows; ++i)
-        if (M->ptr[i + 1] < M->ptr[i])
-            throw Error(NK_ERR_INVALID, std::string("invalid ") + what + " CSR offsets");
-    if (M->ptr[rows] > 0 && (!M->index || !M->value))
-        throw Error(NK_ERR_INVALID, std::string("missing ") + what + " entries");
-}
-
-// Upload a host CSR, check indices on the device, convert to the engine format.
-void upload_matrix(DeviceMatrix &D, const nk_csr *H, bool wide, int vbits, cudaStream_t stream,
-                   DevBuf<int64_t> *keep_ptr = nullptr, DevBuf<int64_t> *keep_idx = nullptr,
-                   DevBuf<double> *keep_val = nullptr) {
-    int64_t nnz = H->ptr[H->rows];
-    DevBuf<int64_t> p(static_cast<size_t>(H->rows + 1)), ix(std::max<int64_t>(1, nnz));
-    DevBuf<double> vv(std::max<int64_t>(1, nnz));
-    cuda_check(cudaMemcpyAsync(p.p, H->ptr, size_t(H->rows + 1) * 8, cudaMemcpyHostToDevice, stream),
-               "ptr upload");
-    if (nnz) {
-        cuda_check(cudaMemcpyAsync(ix.p, H->index, size_t(nnz) * 8, cudaMemcpyHostToDevice, stream),
-                   "index upload");
-        cuda_check(cudaMemcpyAsync(vv.p, H->value, size_t(nnz) * 8, cudaMemcpyHostToDevice, stream),
-                   "value upload");
-        DevBuf<int> bad(1);
-        cuda_check(cudaMemsetAsync(bad.p, 0, sizeof(int), stream), "flag");
-        check_indices<<<grid_for(nnz, 148 * 32), kThreads, 0, stream>>>(nnz, ix.p, vv.p, H->cols,
-                                                                        bad.p);
-        if (vbits == 32)
-            fp32_flags<<<grid_for(nnz, 148 * 32), kThreads, 0, stream>>>(nnz, vv.p, bad.p + 0);
-        int hb = 0;
-        cuda_check(cudaMemcpyAsync(&hb, bad.p, sizeof(int), cudaMemcpyDeviceToHost, stream), "flag");
-        cuda_check(cudaStreamSynchronize(stream), "index check");
-        if (hb)
-            throw Error(NK_ERR_INVALID,
-                        vbits == 32 ? "invalid coefficient/index, or FP32 matrix conversion would "
-                                      "overflow or erase a coefficient; use fp64"
-                                    : "Invalid matrix coefficient/index");
-    }
-    fill_matrix(D, H->rows, H->cols, p.p, ix.p, vv.p, wide, vbits, stream);
-    cuda_check(cudaStreamSynchronize(stream), "matrix upload");
-    if (keep_ptr) {
-        *keep_ptr = std::move(p);
-        *keep_idx = std::move(ix);
-        *keep_val = std::move(vv);
-    }
+template <class Acc, class V, class I> void configure(Engine &E) {
+    constexpr bool F32 = sizeof(Acc) == 4;
+    const void *pk = E.sparse_q ? (const void *)primal_kernel<Acc, V, I, true, F32>
+                                : (const void *)primal_kernel<Acc, V, I, false, F32>;
+    E.grid_p = occupancy_grid(pk, (E.At.nv + 31) / 32);
+    E.grid_d = occupancy_grid((const void *)dual_kernel<Acc, V, I, F32>, (E.A.nv + 31) / 32);
+    E.grid_s = occupancy_grid((const void *)spmv_kernel<V, I>, int64_t(1) << 40);
 }
 
 Engine *create_engine(const nk_csr *Ah, const nk_csr *Qh, const double *hc, const double *hq,
@@ -1264,10 +931,11 @@ Engine *create_engine(const nk_csr *Ah, const nk_csr *Qh, const double *hc, cons
     bool fits32 = m <= INT32_MAX && n <= INT32_MAX && nnz <= INT32_MAX && qnnz <= INT32_MAX;
     if (o->index_bits == 32 && !fits32)
         throw Error(NK_ERR_INVALID, "Model exceeds 32-bit CSR limits");
-    int dev = 0, count = 0;
+    if (m >= INT32_MAX || n >= INT32_MAX)
+        throw Error(NK_ERR_UNSUPPORTED, "more than 2^31 rows or columns");
+    int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
         throw Error(NK_ERR_NO_DEVICE, "no CUDA device");
-    cuda_check(cudaGetDevice(&dev), "device");
     size_t freeb = 0, total = 0;
     cuda_check(cudaMemGetInfo(&freeb, &total), "cudaMemGetInfo");
     // the reference guard (src/cuda.cu:1292-1298)
@@ -1288,31 +956,78 @@ Engine *create_engine(const nk_csr *Ah, const nk_csr *Qh, const double *hc, cons
     E->wide = !fits32 || o->index_bits == 64;
     cuda_check(cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking), "stream");
     cudaStream_t s = E->stream;
-    int vbits = o->precision == NK_PRECISION_FP64 ? 64 : 32;
-    if (sparse_q && o->precision == NK_PRECISION_FP64)
-        vbits = 64;
-    // A, then its transpose from the raw device copy
-    DevBuf<int64_t> rp, ri;
-    DevBuf<double> rv;
-    upload_matrix(E->A, Ah, E->wide, vbits, s, &rp, &ri, &rv);
+    const int vbits = o->precision == NK_PRECISION_FP64 ? 64 : 32;
+
+    // ---- A on the device, its transpose, and the engine orders
+    DevBuf<int64_t> rp, ri, tp, ti;
+    DevBuf<double> rv, tv;
+    upload_raw(Ah, vbits, s, rp, ri, rv);
+    device_transpose(m, n, nnz, rp.p, ri.p, rv.p, tp, ti, tv, s);
+    std::vector<int64_t> aptr(Ah->ptr, Ah->ptr + m + 1), tptr(static_cast<size_t>(n + 1));
+    cuda_check(cudaMemcpy(tptr.data(), tp.p, size_t(n + 1) * 8, cudaMemcpyDeviceToHost), "A^T ptr");
+    std::vector<int64_t> rlen(static_cast<size_t>(m)), clen(static_cast<size_t>(n));
+    for (int64_t i = 0; i < m; ++i)
+        rlen[size_t(i)] = aptr[size_t(i + 1)] - aptr[size_t(i)];
+    for (int64_t j = 0; j < n; ++j)
+        clen[size_t(j)] = tptr[size_t(j + 1)] - tptr[size_t(j)];
+    std::vector<int64_t> rperm = order_by_length_desc(rlen), cperm = order_by_length_desc(clen);
+    std::vector<int64_t> rinv(static_cast<size_t>(m)), cinv(static_cast<size_t>(n));
+    for (int64_t i = 0; i < m; ++i)
+        rinv[size_t(rperm[size_t(i)])] = i;
+    for (int64_t j = 0; j < n; ++j)
+        cinv[size_t(cperm[size_t(j)])] = j;
+    DevBuf<int64_t> d_rinv, d_cinv;
+    upload_vector(E->row_perm, rperm, s);
+    upload_vector(E->col_perm, cperm, s);
+    upload_vector(d_rinv, rinv, s);
+    upload_vector(d_cinv, cinv, s);
     {
-        DevBuf<int64_t> tp, ti;
-        DevBuf<double> tv;
-        device_transpose(m, n, nnz, rp.p, ri.p, rv.p, tp, ti, tv, s);
-        fill_matrix(E->At, n, m, tp.p, ti.p, tv.p, E->wide, vbits, s);
-        cuda_check(cudaStreamSynchronize(s), "transpose convert");
+        // rows of A in engine order, columns mapped to engine columns; entries
+        // keep their CSR order (the CPU's summation order)
+        DevBuf<int64_t> pi;
+        DevBuf<double> pv;
+        auto pptr = permute_device_csr(m, aptr, rp.p, ri.p, rv.p, rperm, E->row_perm.p, d_cinv.p,
+                                       pi, pv, s);
+        build_sell(E->A, m, n, pptr, pi.p, pv.p, E->wide, vbits, s);
     }
-    rp.release();
-    ri.release();
-    rv.release();
-    if (sparse_q)
-        upload_matrix(E->Q, Qh, E->wide, vbits, s);
-    build_schedule(E->A, 0, 0);
-    build_schedule(E->At, 0, 0);
-    if (sparse_q)
-        build_schedule(E->Q, E->At.width, 1 << 30); // Q rows follow A^T's geometry
-    // norms for the QP step safety (src/cpu.cpp:25-42)
+    {
+        // rows of A^T (columns of A) in engine order; the transpose lists every
+        // column's entries by increasing original row, the CPU's order
+        DevBuf<int64_t> pi;
+        DevBuf<double> pv;
+        auto pptr = permute_device_csr(n, tptr, tp.p, ti.p, tv.p, cperm, E->col_perm.p, d_rinv.p,
+                                       pi, pv, s);
+        build_sell(E->At, n, m, pptr, pi.p, pv.p, E->wide, vbits, s);
+    }
+    rp.release(); ri.release(); rv.release(); tp.release(); ti.release(); tv.release();
     if (sparse_q) {
+        DevBuf<int64_t> qp, qi, pi;
+        DevBuf<double> qv, pv;
+        upload_raw(Qh, vbits, s, qp, qi, qv);
+        std::vector<int64_t> qptr_h(Qh->ptr, Qh->ptr + n + 1);
+        auto pptr = permute_device_csr(n, qptr_h, qp.p, qi.p, qv.p, cperm, E->col_perm.p, d_cinv.p,
+                                       pi, pv, s);
+        E->Q.n = n;
+        E->Q.nnz = qnnz;
+        E->Q.wide = E->wide;
+        E->Q.vbits = vbits;
+        upload_vector(E->Q.ptr, pptr, s);
+        E->Q.idx64.alloc(E->wide ? size_t(std::max<int64_t>(1, qnnz)) : 1);
+        E->Q.idx32.alloc(E->wide ? 1 : size_t(std::max<int64_t>(1, qnnz)));
+        E->Q.val64.alloc(vbits == 64 ? size_t(std::max<int64_t>(1, qnnz)) : 1);
+        E->Q.val32.alloc(vbits == 64 ? 1 : size_t(std::max<int64_t>(1, qnnz)));
+        int g = grid_for(qnnz, 148 * 32);
+        if (E->wide && vbits == 64)
+            convert_csr<double, int64_t><<<g, kThreads, 0, s>>>(qnnz, pi.p, pv.p, E->Q.idx64.p, E->Q.val64.p);
+        else if (E->wide)
+            convert_csr<float, int64_t><<<g, kThreads, 0, s>>>(qnnz, pi.p, pv.p, E->Q.idx64.p, E->Q.val32.p);
+        else if (vbits == 64)
+            convert_csr<double, int32_t><<<g, kThreads, 0, s>>>(qnnz, pi.p, pv.p, E->Q.idx32.p, E->Q.val64.p);
+        else
+            convert_csr<float, int32_t><<<g, kThreads, 0, s>>>(qnnz, pi.p, pv.p, E->Q.idx32.p, E->Q.val32.p);
+        cuda_check(cudaGetLastError(), "Q convert");
+        cuda_check(cudaStreamSynchronize(s), "Q build");
+        // norms for the QP step safety (src/cpu.cpp:25-42, src/model.cpp:257-267)
         std::vector<double> cols(static_cast<size_t>(n), 0.0);
         double rowmax = 0;
         for (int64_t i = 0; i < m; ++i) {
@@ -1327,7 +1042,7 @@ Engine *create_engine(const nk_csr *Ah, const nk_csr *Qh, const double *hc, cons
         for (double v : cols)
             colmax = std::max(colmax, v);
         E->a_norm = std::sqrt(rowmax) * std::sqrt(colmax);
-        long double largest = 0; // Model::quadratic_norm_bound, src/model.cpp:257-267
+        long double largest = 0;
         for (int64_t i = 0; i < n; ++i) {
             long double sum = std::abs(hq ? hq[i] : 0.0);
             for (int64_t k = Qh->ptr[i]; k < Qh->ptr[i + 1]; ++k)
@@ -1336,64 +1051,62 @@ Engine *create_engine(const nk_csr *Ah, const nk_csr *Qh, const double *hc, cons
         }
         E->q_norm = std::nextafter(double(largest), INFINITY);
     }
-    auto vec = [&](DevBuf<double> &d, const double *h, int64_t len) {
+
+    // ---- vectors, in engine order
+    auto vec = [&](DevBuf<double> &d, const double *h, int64_t len, const std::vector<int64_t> &perm) {
         d.alloc(std::max<int64_t>(1, len));
-        if (len && h)
-            cuda_check(cudaMemcpyAsync(d.p, h, size_t(len) * 8, cudaMemcpyHostToDevice, s), "vector");
-        else if (len)
+        if (len && h) {
+            std::vector<double> tmp(static_cast<size_t>(len));
+            for (int64_t i = 0; i < len; ++i)
+                tmp[size_t(i)] = h[perm[size_t(i)]];
+            cuda_check(cudaMemcpyAsync(d.p, tmp.data(), size_t(len) * 8, cudaMemcpyHostToDevice, s),
+                       "vector");
+            cuda_check(cudaStreamSynchronize(s), "vector");
+        } else if (len)
             cuda_check(cudaMemsetAsync(d.p, 0, size_t(len) * 8, s), "vector zero");
     };
-    vec(E->c, hc, n);
-    vec(E->q, hq, n);
-    vec(E->lb, hlb, n);
-    vec(E->ub, hub, n);
-    vec(E->rl, hrl, m);
-    vec(E->ru, hru, m);
-    vec(E->x[0], hx0, n);
-    vec(E->x[1], hx0, n);
-    vec(E->y[0], hy0, m);
-    vec(E->y[1], hy0, m);
-    vec(E->xa, nullptr, n);
-    vec(E->ya, nullptr, m);
-    vec(E->ax[0], nullptr, m);
-    vec(E->ax[1], nullptr, m);
+    vec(E->c, hc, n, cperm);
+    vec(E->q, hq, n, cperm);
+    vec(E->lb, hlb, n, cperm);
+    vec(E->ub, hub, n, cperm);
+    vec(E->rl, hrl, m, rperm);
+    vec(E->ru, hru, m, rperm);
+    vec(E->x[0], hx0, n, cperm);
+    vec(E->x[1], hx0, n, cperm);
+    vec(E->y[0], hy0, m, rperm);
+    vec(E->y[1], hy0, m, rperm);
+    vec(E->xa, nullptr, n, cperm);
+    vec(E->ya, nullptr, m, rperm);
+    vec(E->ax[0], nullptr, m, rperm);
+    vec(E->ax[1], nullptr, m, rperm);
+    E->scratch_n.alloc(size_t(std::max<int64_t>(1, n)));
+    E->scratch_m.alloc(size_t(std::max<int64_t>(1, m)));
     if (o->precision == NK_PRECISION_FP32) {
         E->dx32.alloc(std::max<int64_t>(1, n));
         E->y32[0].alloc(std::max<int64_t>(1, m));
         E->y32[1].alloc(std::max<int64_t>(1, m));
         E->dx.alloc(1);
     } else {
-        vec(E->dx, nullptr, n);
+        vec(E->dx, nullptr, n, cperm);
         E->dx32.alloc(1);
         E->y32[0].alloc(1);
         E->y32[1].alloc(1);
     }
     if (E->halpern) {
-        vec(E->anchor_x, hx0, n);
-        vec(E->anchor_y, hy0, m);
-        vec(E->anchor_ax, nullptr, m);
+        vec(E->anchor_x, hx0, n, cperm);
+        vec(E->anchor_y, hy0, m, rperm);
+        vec(E->anchor_ax, nullptr, m, rperm);
     } else {
         E->anchor_x.alloc(1);
         E->anchor_y.alloc(1);
         E->anchor_ax.alloc(1);
     }
-    // grids from occupancy
-    {
-        const void *pk, *dk;
-        if (o->precision == NK_PRECISION_FP32) {
-            pk = E->wide ? (const void *)primal_kernel<float, float, int64_t, int64_t, false, true>
-                         : (const void *)primal_kernel<float, float, int32_t, int32_t, false, true>;
-            dk = E->wide ? (const void *)dual_kernel<float, float, int64_t, int64_t, true>
-                         : (const void *)dual_kernel<float, float, int32_t, int32_t, true>;
-        } else {
-            pk = E->wide ? (const void *)primal_kernel<double, double, int64_t, int64_t, false, false>
-                         : (const void *)primal_kernel<double, double, int32_t, int32_t, false, false>;
-            dk = E->wide ? (const void *)dual_kernel<double, double, int64_t, int64_t, false>
-                         : (const void *)dual_kernel<double, double, int32_t, int32_t, false>;
-        }
-        E->grid_p = occupancy_grid(pk, std::max(1, E->At.nitems));
-        E->grid_d = occupancy_grid(dk, std::max(1, E->A.nitems));
-    }
+    if (o->precision == NK_PRECISION_FP64)
+        E->wide ? configure<double, double, int64_t>(*E) : configure<double, double, int32_t>(*E);
+    else if (o->precision == NK_PRECISION_MIXED)
+        E->wide ? configure<double, float, int64_t>(*E) : configure<double, float, int32_t>(*E);
+    else
+        E->wide ? configure<float, float, int64_t>(*E) : configure<float, float, int32_t>(*E);
     E->part_p.alloc(size_t(E->grid_p));
     E->part_d.alloc(size_t(2 * E->grid_d));
     E->ctl.alloc(1);
@@ -1402,8 +1115,6 @@ Engine *create_engine(const nk_csr *Ah, const nk_csr *Qh, const double *hc, cons
     init.factor = 1;
     init.init_res = INFINITY;
     init.prev_res = INFINITY;
-    init.tau = 0;
-    init.sigma = 0;
     init.flags = (E->adaptive ? 1 : 0) | (E->halpern ? 2 : 0) | (E->residual_restarts ? 4 : 0);
     *E->host_ctl = init;
     E->push_ctl();
@@ -1541,12 +1252,13 @@ nk_status nk_pdhg_schedule_info(nk_pdhg *h, int *a_width, int64_t *a_long, int *
                                 int64_t *at_long, int *a_items, int *at_items) {
     return guard([&] {
         NK_HANDLE
-        *a_width = h->e->A.width;
-        *a_long = h->e->A.long_threshold;
-        *at_width = h->e->At.width;
-        *at_long = h->e->At.long_threshold;
-        *a_items = h->e->A.nitems;
-        *at_items = h->e->At.nitems;
+        // SELL-32: one lane per row; reported: lanes per row, split length, chunks
+        *a_width = 1;
+        *a_long = NK_SPLIT;
+        *at_width = 1;
+        *at_long = NK_SPLIT;
+        *a_items = int((h->e->A.nv + 31) / 32);
+        *at_items = int((h->e->At.nv + 31) / 32);
     });
 }
 int nk_cuda_available(void) {
