@@ -87,6 +87,49 @@ __device__ __forceinline__ bool split_done(double *slots, unsigned *counters, in
     return true;
 }
 
+// Split-region chunk (all 32 lanes hold segments or padding): every lane
+// publishes its segment sum; the leader lane of a row that lies in this chunk
+// adds its segments in order (from init) and gets true with the total; for a
+// row spanning chunks, the lane that completes the row gets true.
+__device__ __forceinline__ bool split_chunk(double *wpart /* this warp's 32 */, double *slots,
+                                           unsigned *counters, int4 sg, int64_t vr, double part,
+                                           double init, double *total) {
+    const int lane = threadIdx.x & 31;
+    wpart[lane] = part;
+    __syncwarp();
+    bool done = false;
+    if (sg.x >= 0) {
+        if (sg.w < 0) {
+            if (vr == sg.y) {
+                double t = init;
+                for (int s = 0; s < sg.z; ++s)
+                    t += wpart[lane + s];
+                *total = t;
+                done = true;
+            }
+        } else {
+            done = split_done(slots, counters, sg, vr, part, init, total);
+        }
+    }
+    __syncwarp();
+    return done;
+}
+
+// The split-region work of one lane: dot product of its segment, then the
+// chunk combine.  Kept out of line so that the register budget of the kernels'
+// main path does not carry it.  init_vec (may be null) gives the row sum's
+// start; on true, *row and *total hold the completed row.
+template <class Acc, class V, class I, class X>
+__device__ __noinline__ bool split_lane(const Sell<V, I> M, int64_t vr, int len,
+                                        const X *__restrict__ x, const double *init_vec,
+                                        double *wpart, int64_t *row, double *total) {
+    const double part = double(sell_dot<Acc, kUnrollSplit>(M, vr, len, Acc(0), x));
+    const int4 sg = M.seg[vr];
+    *row = sg.x;
+    const double init = (sg.x >= 0 && init_vec) ? init_vec[sg.x] : 0.;
+    return split_chunk(wpart, M.slots, M.counters, sg, vr, part, init, total);
+}
+
 // Index of the first SELL chunk of the calling warp and the warp stride of a
 // persistent grid.
 __device__ __forceinline__ int64_t first_chunk() {
@@ -97,10 +140,13 @@ __device__ __forceinline__ int64_t chunk_stride() {
 }
 
 // ------------------------------------------------------------------ primal
-template <class Acc, class V, class I, bool SPARSE_Q, bool FP32G>
+// SPLIT: the matrix has split rows (kernels without them skip that path
+// entirely, which keeps their register footprint small).
+template <class Acc, class V, class I, bool SPARSE_Q, bool FP32G, bool SPLIT>
 __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS)
     primal_kernel(Sell<V, I> At, QCsr<V, I> Q, Vecs v) {
     __shared__ double red[kWarps];
+    __shared__ double wpart[kWarps][32];
     const Control &ctl = *v.ctl;
     double mine = 0;
     bool bad = false;
@@ -137,7 +183,7 @@ __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS)
             if (vr >= At.nv)
                 continue;
             const int len = At.len[vr];
-            if (vr >= At.nsv) {
+            if (!SPLIT || vr >= At.nsv) {
                 const int64_t j = vr - At.nsv + At.nsr;
                 // the epilogue's loads do not depend on the dot product: issue them first
                 const double xj = x[j], cj = v.c[j], qj = v.q[j], lj = v.lb[j], uj = v.ub[j];
@@ -148,17 +194,19 @@ __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS)
                 else // FP64 accumulation starts from c_j, like the CPU loop (src/cpu.cpp:108-111)
                     g = double(sell_dot<Acc>(At, vr, len, Acc(cj), y));
                 finish(j, g, xj, qj, lj, uj, aj);
-            } else {
-                double part;
-                if constexpr (FP32G)
-                    part = double(sell_dot<Acc>(At, vr, len, Acc(0), y32));
-                else
-                    part = double(sell_dot<Acc>(At, vr, len, Acc(0), y));
-                const int4 sg = At.seg[vr];
-                const int64_t j = sg.x;
+            } else if constexpr (SPLIT) { // split region: the whole warp is here
+                int64_t j;
                 double g;
-                if (split_done(At.slots, At.counters, sg, vr, part, v.c[j], &g))
+                bool done;
+                if constexpr (FP32G) // FP32 sums add c_j afterwards, in FP64
+                    done = split_lane<Acc>(At, vr, len, y32, nullptr, wpart[threadIdx.x >> 5], &j, &g);
+                else
+                    done = split_lane<Acc>(At, vr, len, y, v.c, wpart[threadIdx.x >> 5], &j, &g);
+                if (done) {
+                    if constexpr (FP32G)
+                        g = v.c[j] + g;
                     finish(j, g, x[j], v.q[j], v.lb[j], v.ub[j], pending ? v.xa[j] : 0.);
+                }
             }
         }
     }
@@ -218,9 +266,10 @@ __device__ inline void decide(Vecs &v, double p, double d, double c) {
         s.rejected += 1;
 }
 
-template <class Acc, class V, class I, bool FP32G>
+template <class Acc, class V, class I, bool FP32G, bool SPLIT>
 __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS) dual_kernel(Sell<V, I> A, Vecs v) {
     __shared__ double red[kWarps * 3];
+    __shared__ double wpart[kWarps][32];
     __shared__ bool last;
     const Control &ctl = *v.ctl;
     double dy2 = 0, cpl = 0;
@@ -257,7 +306,7 @@ __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS) dual_kernel(Sell<V, I
             if (vr >= A.nv)
                 continue;
             const int len = A.len[vr];
-            if (vr >= A.nsv) {
+            if (!SPLIT || vr >= A.nsv) {
                 const int64_t i = vr - A.nsv + A.nsr;
                 const double yi = y[i], axi = ax[i], rli = v.rl[i], rui = v.ru[i];
                 const double ai = pending ? v.ya[i] : 0.;
@@ -267,16 +316,15 @@ __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS) dual_kernel(Sell<V, I
                 else
                     delta = double(sell_dot<Acc>(A, vr, len, Acc(0), v.dx));
                 finish(i, delta, yi, axi, rli, rui, ai);
-            } else {
-                double part;
-                if constexpr (FP32G)
-                    part = double(sell_dot<Acc>(A, vr, len, Acc(0), v.dx32));
-                else
-                    part = double(sell_dot<Acc>(A, vr, len, Acc(0), v.dx));
-                const int4 sg = A.seg[vr];
-                const int64_t i = sg.x;
+            } else if constexpr (SPLIT) { // split region: the whole warp is here
+                int64_t i;
                 double delta;
-                if (split_done(A.slots, A.counters, sg, vr, part, 0., &delta))
+                bool done;
+                if constexpr (FP32G)
+                    done = split_lane<Acc>(A, vr, len, v.dx32, nullptr, wpart[threadIdx.x >> 5], &i, &delta);
+                else
+                    done = split_lane<Acc>(A, vr, len, v.dx, nullptr, wpart[threadIdx.x >> 5], &i, &delta);
+                if (done)
                     finish(i, delta, y[i], ax[i], v.rl[i], v.ru[i], pending ? v.ya[i] : 0.);
             }
         }
@@ -366,6 +414,7 @@ __global__ void clear_pending(Control *s) { s->pending = 0; }
 template <class V, class I>
 __global__ void __launch_bounds__(kThreads) spmv_kernel(Sell<V, I> M, const double *x,
                                                         double *out) {
+    __shared__ double wpart[kWarps][32];
     const int lane = threadIdx.x & 31;
     for (int64_t ch = first_chunk(); ch * 32 < M.nv; ch += chunk_stride()) {
         const int64_t vr = ch * 32 + lane;
@@ -378,7 +427,7 @@ __global__ void __launch_bounds__(kThreads) spmv_kernel(Sell<V, I> M, const doub
         } else {
             const int4 sg = M.seg[vr];
             double t;
-            if (split_done(M.slots, M.counters, sg, vr, s, 0., &t))
+            if (split_chunk(wpart[threadIdx.x >> 5], M.slots, M.counters, sg, vr, s, 0., &t))
                 out[sg.x] = t;
         }
     }

@@ -20,7 +20,7 @@
 #include <vector>
 
 #ifndef NK_SPLIT
-#define NK_SPLIT 256 // rows with more entries are split into virtual rows of this length
+#define NK_SPLIT 64 // rows with more entries are split into virtual rows of this length
 #endif
 
 namespace nk {
@@ -128,26 +128,43 @@ struct SellPlan {
     std::vector<int32_t> len;
     std::vector<int4> seg;
     int64_t nv = 0, nsv = 0, nsr = 0;
+    int ncounters = 0; // split rows spanning more than one chunk
 };
 
 // Virtual rows and chunks for an engine-order CSR (rows sorted longest first):
 // rows longer than `split` become consecutive segments of at most `split`
-// entries, placed first; chunks of 32 virtual rows are padded to their longest.
+// entries, placed first in whole chunks (a row of at most 32 segments inside
+// one chunk); chunks of 32 virtual rows are padded to their longest.
 SellPlan plan_sell(const std::vector<int64_t> &ptr, int64_t rows, int64_t split) {
     SellPlan P;
     while (P.nsr < rows && ptr[size_t(P.nsr + 1)] - ptr[size_t(P.nsr)] > split)
         ++P.nsr;
+    auto pad_to_chunk = [&]() {
+        while (P.len.size() % 32) {
+            P.len.push_back(0);
+            P.src.push_back(0);
+            P.seg.push_back(make_int4(-1, 0, 0, -1));
+        }
+    };
+    int ncounters = 0;
     for (int64_t r = 0; r < P.nsr; ++r) {
         int64_t L = ptr[size_t(r + 1)] - ptr[size_t(r)];
-        int nseg = int((L + split - 1) / split);
+        int64_t nseg = (L + split - 1) / split;
+        bool local = nseg <= 32;
+        // a row that fits one chunk never straddles two
+        if (local && int64_t(P.len.size() % 32) + nseg > 32)
+            pad_to_chunk();
         int first = int(P.len.size());
-        for (int s = 0; s < nseg; ++s) {
-            P.len.push_back(int32_t(std::min<int64_t>(split, L - int64_t(s) * split)));
-            P.src.push_back(ptr[size_t(r)] + int64_t(s) * split);
-            P.seg.push_back(make_int4(int(r), first, nseg, int(r)));
+        int counter = local ? -1 : ncounters++;
+        for (int64_t s = 0; s < nseg; ++s) {
+            P.len.push_back(int32_t(std::min<int64_t>(split, L - s * split)));
+            P.src.push_back(ptr[size_t(r)] + s * split);
+            P.seg.push_back(make_int4(int(r), first, int(nseg), counter));
         }
     }
+    pad_to_chunk(); // split segments fill whole chunks
     P.nsv = int64_t(P.len.size());
+    P.ncounters = ncounters;
     for (int64_t r = P.nsr; r < rows; ++r) {
         P.len.push_back(int32_t(ptr[size_t(r + 1)] - ptr[size_t(r)]));
         P.src.push_back(ptr[size_t(r)]);
@@ -190,7 +207,7 @@ void build_sell(SellMatrix &M, int64_t rows, int64_t cols, const std::vector<int
     DevBuf<int64_t> src;
     upload_vector(src, P.src, s);
     M.slots.alloc(size_t(std::max<int64_t>(1, P.nsv)));
-    M.counters.alloc(size_t(std::max<int64_t>(1, P.nsr)));
+    M.counters.alloc(size_t(std::max(1, P.ncounters)));
     cuda_check(cudaMemsetAsync(M.counters.p, 0, M.counters.bytes(), s), "split counters");
     size_t total = size_t(std::max<int64_t>(1, M.padded));
     if (wide) {
@@ -426,13 +443,21 @@ struct Engine {
         auto qm = Q.view<V, I>();
         if (ev[0])
             cudaEventRecord(ev[0], stream);
-        if (sparse_q)
-            primal_kernel<Acc, V, I, true, F32><<<grid_p, kThreads, 0, stream>>>(at, qm, v);
+        const bool ps = At.nsv > 0, ds = A.nsv > 0;
+        if (sparse_q && ps)
+            primal_kernel<Acc, V, I, true, F32, true><<<grid_p, kThreads, 0, stream>>>(at, qm, v);
+        else if (sparse_q)
+            primal_kernel<Acc, V, I, true, F32, false><<<grid_p, kThreads, 0, stream>>>(at, qm, v);
+        else if (ps)
+            primal_kernel<Acc, V, I, false, F32, true><<<grid_p, kThreads, 0, stream>>>(at, qm, v);
         else
-            primal_kernel<Acc, V, I, false, F32><<<grid_p, kThreads, 0, stream>>>(at, qm, v);
+            primal_kernel<Acc, V, I, false, F32, false><<<grid_p, kThreads, 0, stream>>>(at, qm, v);
         if (ev[1])
             cudaEventRecord(ev[1], stream);
-        dual_kernel<Acc, V, I, F32><<<grid_d, kThreads, 0, stream>>>(a, v);
+        if (ds)
+            dual_kernel<Acc, V, I, F32, true><<<grid_d, kThreads, 0, stream>>>(a, v);
+        else
+            dual_kernel<Acc, V, I, F32, false><<<grid_d, kThreads, 0, stream>>>(a, v);
         if (ev[2])
             cudaEventRecord(ev[2], stream);
         if (halpern)
@@ -900,10 +925,15 @@ int occupancy_grid(const void *kernel, int64_t chunks) {
 
 template <class Acc, class V, class I> void configure(Engine &E) {
     constexpr bool F32 = sizeof(Acc) == 4;
-    const void *pk = E.sparse_q ? (const void *)primal_kernel<Acc, V, I, true, F32>
-                                : (const void *)primal_kernel<Acc, V, I, false, F32>;
+    const bool ps = E.At.nsv > 0, ds = E.A.nsv > 0;
+    const void *pk = E.sparse_q ? (ps ? (const void *)primal_kernel<Acc, V, I, true, F32, true>
+                                      : (const void *)primal_kernel<Acc, V, I, true, F32, false>)
+                                : (ps ? (const void *)primal_kernel<Acc, V, I, false, F32, true>
+                                      : (const void *)primal_kernel<Acc, V, I, false, F32, false>);
+    const void *dk = ds ? (const void *)dual_kernel<Acc, V, I, F32, true>
+                        : (const void *)dual_kernel<Acc, V, I, F32, false>;
     E.grid_p = occupancy_grid(pk, (E.At.nv + 31) / 32);
-    E.grid_d = occupancy_grid((const void *)dual_kernel<Acc, V, I, F32>, (E.A.nv + 31) / 32);
+    E.grid_d = occupancy_grid(dk, (E.A.nv + 31) / 32);
     E.grid_s = occupancy_grid((const void *)spmv_kernel<V, I>, int64_t(1) << 40);
 }
 

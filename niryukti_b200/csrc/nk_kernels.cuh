@@ -11,7 +11,16 @@ constexpr int kWarps = kThreads / 32;
 
 // Streaming loads for single-use matrix data (evict-first), cached loads for
 // the gathered vector, which stays resident in L2.
-template <class T> __device__ __forceinline__ T stream_load(const T *p) { return __ldcs(p); }
+#ifndef NK_STREAM_HINT
+#define NK_STREAM_HINT 1 // 1: evict-first loads for matrix entries, 0: default caching
+#endif
+template <class T> __device__ __forceinline__ T stream_load(const T *p) {
+#if NK_STREAM_HINT
+    return __ldcs(p);
+#else
+    return *p;
+#endif
+}
 template <class T> __device__ __forceinline__ T gather_load(const T *p) { return __ldg(p); }
 
 // Deterministic CTA reduction of NV doubles (fixed tree); result in thread 0.

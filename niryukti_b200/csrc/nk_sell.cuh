@@ -11,11 +11,13 @@
 // the sum has the order and rounding of a sequential CPU loop.
 //
 // Rows longer than the split length are cut into segments ("virtual rows") of
-// at most that length; the segments of split rows come first.  Each segment's
-// sum goes to a slot, and the last segment of a row to arrive (an atomic
-// counter) adds the slots in order and runs the epilogue, so the result does
-// not depend on timing.  Padding entries are never read (lane loops stop at
-// their own length).
+// at most that length; the segments of split rows come first, in whole chunks.
+// A row of at most 32 segments lies inside one chunk: its warp adds the
+// segment sums in order through shared memory (the row's first lane leads).
+// Longer rows span chunks: each segment's sum goes to a slot, and the last
+// segment of the row to arrive (an atomic counter) adds the slots in order.
+// Either way the result does not depend on timing.  Padding entries and padding
+// virtual rows are never read (lane loops stop at their own length).
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
@@ -25,7 +27,14 @@ namespace nk {
 #ifndef NK_UNROLL
 #define NK_UNROLL 4
 #endif
-constexpr int kUnroll = NK_UNROLL; // independent loads in flight per lane
+#ifndef NK_UNROLL_SPLIT
+#define NK_UNROLL_SPLIT 4
+#endif
+#ifndef NK_REMAINDER_BATCH
+#define NK_REMAINDER_BATCH 0 // 1: remainder entries as one predicated batch
+#endif
+constexpr int kUnroll = NK_UNROLL;            // independent loads in flight per lane
+constexpr int kUnrollSplit = NK_UNROLL_SPLIT; // the same for split-row segments
 
 template <class V, class I> struct Sell {
     const int64_t *cptr;   // nchunks + 1 element offsets
@@ -35,16 +44,18 @@ template <class V, class I> struct Sell {
     int64_t nv;            // virtual rows
     int64_t nsv;           // leading virtual rows that are segments of split rows
     int64_t nsr;           // leading real rows that were split
-    const int4 *seg;       // per split segment: {real row, first segment, segments, counter}
+    const int4 *seg;       // per split segment: {real row (-1: padding), first segment,
+                           //   segments, counter (-1: the row lies in one chunk)}
     double *slots;         // per split segment: partial sum
     unsigned *counters;    // per split row: arrivals (reset by the last one)
 };
 
 // Sequential dot product of virtual row v (entries in CSR order) starting
-// from acc; kUnroll entries' loads are issued before their products are added.
-template <class Acc, class V, class I, class X>
+// from acc; U entries' loads are issued before their products are added.
+template <class Acc, int U = kUnroll, class V, class I, class X>
 __device__ __forceinline__ Acc sell_dot(const Sell<V, I> &M, int64_t v, int len, Acc acc,
                                         const X *__restrict__ x) {
+    constexpr int kUnroll = U;
     const int64_t base = M.cptr[v >> 5] + (v & 31);
     const I *ip = M.idx + base;
     const V *vp = M.val + base;
@@ -65,9 +76,31 @@ __device__ __forceinline__ Acc sell_dot(const Sell<V, I> &M, int64_t v, int len,
         for (int u = 0; u < kUnroll; ++u)
             acc = acc + Acc(w[u]) * Acc(g[u]);
     }
+#if NK_REMAINDER_BATCH
+    if (k < len) { // remainder: one predicated batch of independent loads
+        I j[kUnroll];
+        V w[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u)
+            if (k + u < len) {
+                j[u] = stream_load(ip + int64_t(k + u) * 32);
+                w[u] = stream_load(vp + int64_t(k + u) * 32);
+            }
+        X g[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u)
+            if (k + u < len)
+                g[u] = gather_load(x + j[u]);
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u)
+            if (k + u < len)
+                acc = acc + Acc(w[u]) * Acc(g[u]);
+    }
+#else
     for (; k < len; ++k)
         acc = acc + Acc(stream_load(vp + int64_t(k) * 32)) *
                         Acc(gather_load(x + stream_load(ip + int64_t(k) * 32)));
+#endif
     return acc;
 }
 
