@@ -119,6 +119,10 @@ nk_status nk_pdhg_stats(nk_pdhg *h, int64_t *trials, int64_t *device_bytes);
  * + decision) kernels in milliseconds.  The trials advance the iterate. */
 nk_status nk_pdhg_profile(nk_pdhg *h, int count, double tau, double sigma, double *ms_primal,
                           double *ms_dual);
+/* Profiling (no reference counterpart): mean duration in milliseconds of `reps`
+ * plain SpMVs (no fused epilogue) with A (which = 0, input x) or A^T (which = 1,
+ * input y) on the resident iterate; results go to scratch, iterates unchanged. */
+nk_status nk_pdhg_time_spmv(nk_pdhg *h, int which, int reps, double *ms);
 /* The CUDA stream (cudaStream_t) every kernel and copy of this handle runs on,
  * for callers that time the engine with CUDA events. */
 nk_status nk_pdhg_stream(nk_pdhg *h, void **stream);

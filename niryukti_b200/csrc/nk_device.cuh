@@ -24,6 +24,9 @@
 #ifndef NK_MIN_BLOCKS
 #define NK_MIN_BLOCKS 4 // CTAs per SM the fused kernels are register-bounded for
 #endif
+#ifndef NK_PREFETCH
+#define NK_PREFETCH 1 // 1: load a row's epilogue vectors before its dot product
+#endif
 
 namespace nk {
 
@@ -88,9 +91,12 @@ __device__ __forceinline__ bool split_done(double *slots, unsigned *counters, in
 }
 
 // Split-region chunk (all 32 lanes hold segments or padding): every lane
-// publishes its segment sum; the leader lane of a row that lies in this chunk
-// adds its segments in order (from init) and gets true with the total; for a
-// row spanning chunks, the lane that completes the row gets true.
+// publishes its segment sum.  The leader lane of a row that lies in this chunk
+// adds its segments in order (from init).  For a row spanning chunks, each
+// segment sum goes to a slot and the lane whose atomic arrival completes the
+// row gets the total: its warp adds the row's slots cooperatively (lane-strided
+// partial sums and a fixed shuffle tree, so the result is deterministic).  On
+// true, *total holds the completed row of the calling lane.
 __device__ __forceinline__ bool split_chunk(double *wpart /* this warp's 32 */, double *slots,
                                            unsigned *counters, int4 sg, int64_t vr, double part,
                                            double init, double *total) {
@@ -98,17 +104,37 @@ __device__ __forceinline__ bool split_chunk(double *wpart /* this warp's 32 */, 
     wpart[lane] = part;
     __syncwarp();
     bool done = false;
-    if (sg.x >= 0) {
-        if (sg.w < 0) {
-            if (vr == sg.y) {
-                double t = init;
-                for (int s = 0; s < sg.z; ++s)
-                    t += wpart[lane + s];
-                *total = t;
-                done = true;
-            }
-        } else {
-            done = split_done(slots, counters, sg, vr, part, init, total);
+    if (sg.x >= 0 && sg.w < 0 && vr == sg.y) {
+        double t = init;
+        for (int s = 0; s < sg.z; ++s)
+            t += wpart[lane + s];
+        *total = t;
+        done = true;
+    }
+    bool last = false;
+    if (sg.x >= 0 && sg.w >= 0) {
+        slots[vr] = part;
+        __threadfence();
+        last = atomicAdd(&counters[sg.w], 1u) == unsigned(sg.z - 1);
+    }
+    unsigned finishers = __ballot_sync(0xffffffffu, last);
+    if (finishers)
+        __threadfence();
+    while (finishers) {
+        const int b = __ffs(finishers) - 1;
+        finishers &= finishers - 1;
+        const int first = __shfl_sync(0xffffffffu, sg.y, b);
+        const int nseg = __shfl_sync(0xffffffffu, sg.z, b);
+        double acc = 0;
+        for (int s = lane; s < nseg; s += 32)
+            acc += __ldcg(slots + first + s);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+            acc += __shfl_xor_sync(0xffffffffu, acc, off);
+        if (lane == b) {
+            *total = init + acc;
+            counters[sg.w] = 0;
+            done = true;
         }
     }
     __syncwarp();
@@ -185,15 +211,22 @@ __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS)
             const int len = At.len[vr];
             if (!SPLIT || vr >= At.nsv) {
                 const int64_t j = vr - At.nsv + At.nsr;
-                // the epilogue's loads do not depend on the dot product: issue them first
+#if NK_PREFETCH // the epilogue's loads do not depend on the dot product: issue them first
                 const double xj = x[j], cj = v.c[j], qj = v.q[j], lj = v.lb[j], uj = v.ub[j];
                 const double aj = pending ? v.xa[j] : 0.;
+#else
+                const double cj = v.c[j];
+#endif
                 double g;
                 if constexpr (FP32G)
                     g = cj + double(sell_dot<Acc>(At, vr, len, Acc(0), y32));
                 else // FP64 accumulation starts from c_j, like the CPU loop (src/cpu.cpp:108-111)
                     g = double(sell_dot<Acc>(At, vr, len, Acc(cj), y));
+#if NK_PREFETCH
                 finish(j, g, xj, qj, lj, uj, aj);
+#else
+                finish(j, g, x[j], v.q[j], v.lb[j], v.ub[j], pending ? v.xa[j] : 0.);
+#endif
             } else if constexpr (SPLIT) { // split region: the whole warp is here
                 int64_t j;
                 double g;
@@ -308,14 +341,20 @@ __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS) dual_kernel(Sell<V, I
             const int len = A.len[vr];
             if (!SPLIT || vr >= A.nsv) {
                 const int64_t i = vr - A.nsv + A.nsr;
+#if NK_PREFETCH
                 const double yi = y[i], axi = ax[i], rli = v.rl[i], rui = v.ru[i];
                 const double ai = pending ? v.ya[i] : 0.;
+#endif
                 double delta;
                 if constexpr (FP32G)
                     delta = double(sell_dot<Acc>(A, vr, len, Acc(0), v.dx32));
                 else
                     delta = double(sell_dot<Acc>(A, vr, len, Acc(0), v.dx));
+#if NK_PREFETCH
                 finish(i, delta, yi, axi, rli, rui, ai);
+#else
+                finish(i, delta, y[i], ax[i], v.rl[i], v.ru[i], pending ? v.ya[i] : 0.);
+#endif
             } else if constexpr (SPLIT) { // split region: the whole warp is here
                 int64_t i;
                 double delta;
@@ -421,7 +460,7 @@ __global__ void __launch_bounds__(kThreads) spmv_kernel(Sell<V, I> M, const doub
         if (vr >= M.nv)
             continue;
         const int len = M.len[vr];
-        const double s = sell_dot<double>(M, vr, len, 0., x);
+        const double s = sell_dot_pipelined<double>(M, vr, len, 0., x);
         if (vr >= M.nsv) {
             out[vr - M.nsv + M.nsr] = s;
         } else {

@@ -22,6 +22,10 @@
 #ifndef NK_SPLIT
 #define NK_SPLIT 64 // rows with more entries are split into virtual rows of this length
 #endif
+#ifndef NK_SPLIT_MAX
+#define NK_SPLIT_MAX 256 // longest segment of a row that spans several chunks
+#endif
+constexpr int64_t kSplitMax = NK_SPLIT_MAX;
 
 namespace nk {
 
@@ -132,9 +136,10 @@ struct SellPlan {
 };
 
 // Virtual rows and chunks for an engine-order CSR (rows sorted longest first):
-// rows longer than `split` become consecutive segments of at most `split`
-// entries, placed first in whole chunks (a row of at most 32 segments inside
-// one chunk); chunks of 32 virtual rows are padded to their longest.
+// rows longer than `split` become consecutive segments, placed first in whole
+// chunks -- a row of up to 32*kSplitMax entries as at most 32 equal segments
+// inside one chunk, a longer row as segments of kSplitMax entries -- and chunks
+// of 32 virtual rows are padded to their longest.
 SellPlan plan_sell(const std::vector<int64_t> &ptr, int64_t rows, int64_t split) {
     SellPlan P;
     while (P.nsr < rows && ptr[size_t(P.nsr + 1)] - ptr[size_t(P.nsr)] > split)
@@ -149,16 +154,20 @@ SellPlan plan_sell(const std::vector<int64_t> &ptr, int64_t rows, int64_t split)
     int ncounters = 0;
     for (int64_t r = 0; r < P.nsr; ++r) {
         int64_t L = ptr[size_t(r + 1)] - ptr[size_t(r)];
-        int64_t nseg = (L + split - 1) / split;
-        bool local = nseg <= 32;
-        // a row that fits one chunk never straddles two
+        // rows of up to 32 * kSplitMax entries stay inside one chunk: at most 32
+        // segments of equal length (combined by their warp); longer rows span
+        // chunks in segments of kSplitMax (combined through slots)
+        bool local = L <= 32 * kSplitMax;
+        int64_t nseg = local ? std::min<int64_t>(32, (L + split - 1) / split)
+                             : (L + kSplitMax - 1) / kSplitMax;
+        int64_t seglen = (L + nseg - 1) / nseg;
         if (local && int64_t(P.len.size() % 32) + nseg > 32)
-            pad_to_chunk();
+            pad_to_chunk(); // never straddle two chunks
         int first = int(P.len.size());
         int counter = local ? -1 : ncounters++;
         for (int64_t s = 0; s < nseg; ++s) {
-            P.len.push_back(int32_t(std::min<int64_t>(split, L - s * split)));
-            P.src.push_back(ptr[size_t(r)] + s * split);
+            P.len.push_back(int32_t(std::min<int64_t>(seglen, L - s * seglen)));
+            P.src.push_back(ptr[size_t(r)] + s * seglen);
             P.seg.push_back(make_int4(int(r), first, int(nseg), counter));
         }
     }
@@ -899,6 +908,37 @@ struct Engine {
         *ms_dual = td / count;
     }
 
+    // Mean duration (ms) of `reps` plain SpMVs with A (which = 0: A x into Ax) or
+    // A^T (which = 1: A^T y into dx's buffer), timed with events on the stream.
+    // Leaves the iterates untouched (the products go to scratch buffers).
+    double time_spmv(int which, int reps) {
+        if (reps <= 0)
+            throw Error(NK_ERR_INVALID, "reps must be positive");
+        if (!mon_ax.p) {
+            mon_ax.alloc(std::max<int64_t>(1, m));
+            mon_aty.alloc(std::max<int64_t>(1, n));
+        }
+        sync_ctl();
+        int cur = host_ctl->cur;
+        cudaEvent_t a, b;
+        cuda_check(cudaEventCreate(&a), "event");
+        cuda_check(cudaEventCreate(&b), "event");
+        cudaEventRecord(a, stream);
+        for (int r = 0; r < reps; ++r) {
+            if (which == 0)
+                spmv(A, x[cur].p, mon_ax.p);
+            else
+                spmv(At, y[cur].p, mon_aty.p);
+        }
+        cudaEventRecord(b, stream);
+        cudaEventSynchronize(b);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        return double(ms) / reps;
+    }
+
     size_t device_bytes() const {
         size_t b = A.device_bytes() + At.device_bytes() + Q.device_bytes();
         for (auto *d : {&c, &q, &lb, &ub, &rl, &ru, &x[0], &x[1], &y[0], &y[1], &ax[0], &ax[1],
@@ -1270,6 +1310,14 @@ nk_status nk_pdhg_profile(nk_pdhg *h, int count, double tau, double sigma, doubl
     return guard([&] {
         NK_HANDLE
         h->e->profile(count, tau, sigma, ms_primal, ms_dual);
+    });
+}
+nk_status nk_pdhg_time_spmv(nk_pdhg *h, int which, int reps, double *ms) {
+    return guard([&] {
+        NK_HANDLE
+        if (which != 0 && which != 1)
+            throw nk::Error(NK_ERR_INVALID, "which must be 0 (A) or 1 (A^T)");
+        *ms = h->e->time_spmv(which, reps);
     });
 }
 nk_status nk_pdhg_stream(nk_pdhg *h, void **stream) {

@@ -30,9 +30,6 @@ namespace nk {
 #ifndef NK_UNROLL_SPLIT
 #define NK_UNROLL_SPLIT 4
 #endif
-#ifndef NK_REMAINDER_BATCH
-#define NK_REMAINDER_BATCH 0 // 1: remainder entries as one predicated batch
-#endif
 constexpr int kUnroll = NK_UNROLL;            // independent loads in flight per lane
 constexpr int kUnrollSplit = NK_UNROLL_SPLIT; // the same for split-row segments
 
@@ -52,55 +49,77 @@ template <class V, class I> struct Sell {
 
 // Sequential dot product of virtual row v (entries in CSR order) starting
 // from acc; U entries' loads are issued before their products are added.
+// Used inside the fused PDHG kernels, where registers are scarce.
 template <class Acc, int U = kUnroll, class V, class I, class X>
 __device__ __forceinline__ Acc sell_dot(const Sell<V, I> &M, int64_t v, int len, Acc acc,
                                         const X *__restrict__ x) {
-    constexpr int kUnroll = U;
     const int64_t base = M.cptr[v >> 5] + (v & 31);
     const I *ip = M.idx + base;
     const V *vp = M.val + base;
     int k = 0;
-    for (; k + kUnroll <= len; k += kUnroll) {
-        I j[kUnroll];
-        V w[kUnroll];
+    for (; k + U <= len; k += U) {
+        I j[U];
+        V w[U];
 #pragma unroll
-        for (int u = 0; u < kUnroll; ++u) {
+        for (int u = 0; u < U; ++u) {
             j[u] = stream_load(ip + int64_t(k + u) * 32);
             w[u] = stream_load(vp + int64_t(k + u) * 32);
         }
-        X g[kUnroll];
+        X g[U];
 #pragma unroll
-        for (int u = 0; u < kUnroll; ++u)
+        for (int u = 0; u < U; ++u)
             g[u] = gather_load(x + j[u]);
 #pragma unroll
-        for (int u = 0; u < kUnroll; ++u)
+        for (int u = 0; u < U; ++u)
             acc = acc + Acc(w[u]) * Acc(g[u]);
     }
-#if NK_REMAINDER_BATCH
-    if (k < len) { // remainder: one predicated batch of independent loads
-        I j[kUnroll];
-        V w[kUnroll];
-#pragma unroll
-        for (int u = 0; u < kUnroll; ++u)
-            if (k + u < len) {
-                j[u] = stream_load(ip + int64_t(k + u) * 32);
-                w[u] = stream_load(vp + int64_t(k + u) * 32);
-            }
-        X g[kUnroll];
-#pragma unroll
-        for (int u = 0; u < kUnroll; ++u)
-            if (k + u < len)
-                g[u] = gather_load(x + j[u]);
-#pragma unroll
-        for (int u = 0; u < kUnroll; ++u)
-            if (k + u < len)
-                acc = acc + Acc(w[u]) * Acc(g[u]);
-    }
-#else
     for (; k < len; ++k)
         acc = acc + Acc(stream_load(vp + int64_t(k) * 32)) *
                         Acc(gather_load(x + stream_load(ip + int64_t(k) * 32)));
-#endif
+    return acc;
+}
+
+// The same sum, software-pipelined: the gathers of block b are issued, then the
+// index/value loads of block b+1, and only then are block b's products added,
+// so each block costs about one memory round trip instead of two.  It needs
+// more registers; the plain SpMV kernel uses it.
+template <class Acc, int U = kUnroll, class V, class I, class X>
+__device__ __forceinline__ Acc sell_dot_pipelined(const Sell<V, I> &M, int64_t v, int len, Acc acc,
+                                                  const X *__restrict__ x) {
+    if (len <= 0)
+        return acc;
+    const int64_t base = M.cptr[v >> 5] + (v & 31);
+    const I *ip = M.idx + base;
+    const V *vp = M.val + base;
+    I j[U];
+    V w[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+        if (u < len) {
+            j[u] = stream_load(ip + int64_t(u) * 32);
+            w[u] = stream_load(vp + int64_t(u) * 32);
+        }
+    for (int k = 0; k < len; k += U) {
+        X g[U];
+        V wc[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (k + u < len) {
+                g[u] = gather_load(x + j[u]);
+                wc[u] = w[u];
+            }
+        const int kn = k + U;
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (kn + u < len) {
+                j[u] = stream_load(ip + int64_t(kn + u) * 32);
+                w[u] = stream_load(vp + int64_t(kn + u) * 32);
+            }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (k + u < len)
+                acc = acc + Acc(wc[u]) * Acc(g[u]);
+    }
     return acc;
 }
 

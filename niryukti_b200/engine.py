@@ -77,6 +77,7 @@ def library() -> C.CDLL:
     L.nk_pdhg_schedule_info.argtypes = [C.c_void_p, C.POINTER(C.c_int), _I, C.POINTER(C.c_int),
                                         _I, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.nk_pdhg_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+    L.nk_pdhg_time_spmv.argtypes = [C.c_void_p, C.c_int, C.c_int, _D]
     L.nk_cuda_available.restype = C.c_int
     L.nk_cuda_description.argtypes = [C.c_char_p, C.c_int]
     L.nk_hardware_info.argtypes = [C.POINTER(C.c_int), _D, _D]
@@ -224,6 +225,13 @@ class PdhgBackend:
         check(self._L.nk_pdhg_profile(self._h, int(count), float(tau), float(sigma),
                                       C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    def time_spmv(self, which: str, reps: int = 20) -> float:
+        """Mean ms of a plain SpMV with A ("A") or A^T ("At") on the resident iterate."""
+        v = C.c_double()
+        check(self._L.nk_pdhg_time_spmv(self._h, {"A": 0, "At": 1}[which], int(reps),
+                                        C.byref(v)))
+        return v.value
 
     def stream(self) -> int:
         """Raw cudaStream_t of this handle (for CUDA-event timing)."""

@@ -247,3 +247,42 @@ def test_fixed_step_nonfinite_is_an_error(gpu):
         for _ in range(5):
             g.advance(10, 1e10, 1e10)
     assert "stalled or produced nonfinite" in str(e.value)
+
+
+def test_very_long_rows_and_columns_parity(gpu, oracle):
+    """A row of 20000 entries (split across chunks, combined through slots) and a
+    dense column (a long row of A^T), against the oracle."""
+    rng = np.random.default_rng(17)
+    n, m = 20000, 300
+    rows = [np.zeros(n, dtype=np.int64)]          # row 0: every column
+    cols = [np.arange(n, dtype=np.int64)]
+    for i in range(1, m):
+        k = rng.integers(2, 12)
+        rows.append(np.full(k, i, dtype=np.int64))
+        cols.append(np.sort(rng.choice(n, k, replace=False)))
+    r = np.concatenate(rows)
+    c = np.concatenate(cols)
+    dense_col = 7                                   # column 7 in every row
+    extra = np.arange(1, m)
+    keep = ~np.isin(extra, r[c == dense_col])
+    r = np.concatenate([r, extra[keep]])
+    c = np.concatenate([c, np.full(keep.sum(), dense_col)])
+    v = rng.standard_normal(r.size)
+    order = np.lexsort((c, r))
+    r, c, v = r[order], c[order], v[order]
+    ptr = np.zeros(m + 1, dtype=np.int64)
+    np.cumsum(np.bincount(r, minlength=m), out=ptr[1:])
+    x0 = rng.uniform(0, 1, n)
+    model = synth.Model(m=m, n=n, ptr=ptr, idx=c, val=v, c=rng.standard_normal(n), q=np.zeros(n),
+                        lb=np.zeros(n), ub=np.ones(n), rl=np.full(m, -np.inf), ru=np.zeros(m))
+    model.ru = synth.csr_matvec(ptr, c, v, x0, m) + 0.5
+    cpu = oracle.model(model).backend(np.zeros(n), np.zeros(m), adaptive=True)
+    for graphs in (False, True):
+        g = gpu.PdhgBackend(model, adaptive=True, graphs=graphs)
+        done = 0
+        c2 = oracle.model(model).backend(np.zeros(n), np.zeros(m), adaptive=True)
+        for _ in range(3):
+            done = advance_to(g, done + c2.advance(5, 0.001, 0.001), 0.001, 0.001, done)
+            assert g.rejected_steps() == c2.rejected_steps()
+            for u, w in zip(g.candidates(), c2.candidates()):
+                near(u, w, 1e-9)
