@@ -130,6 +130,101 @@ nk_status nk_pdhg_stream(nk_pdhg *h, void **stream);
 nk_status nk_pdhg_schedule_info(nk_pdhg *h, int *a_width, int64_t *a_long, int *at_width,
                                 int64_t *at_long, int *a_items, int *at_items);
 
+/* ------------------------------------------------------------------ solve
+ * Device-resident continuous solve: the reference's solve_continuous for
+ * method "pdhg" (src/solver.cpp:213-780) -- presolve and scaling on the host
+ * (prepare, src/preprocess.cpp:133-346, bit-identical), the PDHG iterations,
+ * candidate evaluation, restarts and primal-weight updates on the GPU, and
+ * the reference's outward-rounded Verifier (src/verify.cpp:103-244) on the
+ * host to certify termination.  Polishing and the Halpern methods stay with
+ * the reference's own driver (which reaches this engine through nk_pdhg_*). */
+
+/* Termination status (the reference's Result::status strings). */
+#define NK_SOLVE_OPTIMAL 0
+#define NK_SOLVE_INFEASIBLE 1
+#define NK_SOLVE_UNBOUNDED 2
+#define NK_SOLVE_ITERATION_LIMIT 3
+#define NK_SOLVE_TIME_LIMIT 4
+#define NK_SOLVE_NUMERICAL_ERROR 5
+
+/* The continuous part of vantage::Model (include/vantage/vantage.hpp:26-39):
+ * minimise offset + c'x + 1/2 sum q_j x_j^2 + 1/2 x'Qx
+ * subject to rl <= A x <= ru, lb <= x <= ub.  Q (n x n) may have rows = 0. */
+typedef struct {
+    nk_csr A, Q;
+    const double *c, *q, *lb, *ub, *rl, *ru;
+    double offset;
+} nk_model;
+
+/* vantage::Options fields the PDHG path reads (include/vantage/vantage.hpp:41-60);
+ * nk_solve_defaults() fills the reference's defaults. */
+typedef struct {
+    double tol;               /* relative KKT tolerance (1e-6) */
+    double time_limit;        /* seconds (60) */
+    int64_t iteration_limit;  /* accepted iterations (100000) */
+    int check_every;          /* iterations between candidate checks (100) */
+    int presolve;             /* 1 */
+    int scaling_combined;     /* 0 = "ruiz", 1 = "combined" */
+    int scaling_passes;       /* 5 */
+    int adaptive;             /* adaptive steps (1) */
+    int restart;              /* restarts (1) */
+    int graphs;               /* replay trials from CUDA graphs (1) */
+    int index_bits;           /* 0, 32 or 64 */
+    int precision;            /* NK_PRECISION_* of the first phase (FP64) */
+    int refine;               /* after a reduced-precision phase, finish in FP64 (1) */
+    double phase_tol;         /* target of the reduced-precision phase (0: 10 * tol) */
+    int verbose;              /* per-check line on stderr (0) */
+    const double *initial_x;  /* optional, n entries */
+    const double *initial_y;  /* optional, m entries */
+} nk_solve_options;
+
+/* vantage::Result fields of the continuous path (include/vantage/vantage.hpp:112-140). */
+typedef struct {
+    int status;                 /* NK_SOLVE_* */
+    int64_t iterations, restarts, rejected_steps, weight_updates;
+    int64_t device_checks, host_checks, removed_rows, removed_columns;
+    int64_t phase_iterations;   /* iterations of the reduced-precision phase */
+    int64_t refine_iterations;  /* iterations of the FP64 refinement */
+    double seconds, preprocess_seconds, transfer_seconds, iteration_seconds,
+        verification_seconds, phase_seconds;
+    /* certified accuracy of the returned point (Verifier::evaluate) */
+    double objective, kkt, primal, dual, gap, lower_bound;
+    /* accuracy of the reduced-precision phase's best point (no safe bound) */
+    double phase_objective, phase_kkt, phase_primal, phase_dual, phase_gap;
+} nk_solve_result;
+
+/* prepare(model, options) -- src/preprocess.cpp:133-346: presolve (fixed and
+ * unused columns, empty, redundant and duplicate rows) and Ruiz / combined
+ * scaling, bit-identical to the reference.  dims = {rows, cols, nnz, qnnz,
+ * failure}: failure 0 none, 1 INFEASIBLE (presolve proof). */
+typedef struct nk_prepared nk_prepared;
+nk_status nk_prepare(const nk_model *model, int presolve, int scaling_combined, int scaling_passes,
+                     nk_prepared **out);
+void nk_prepared_free(nk_prepared *p);
+nk_status nk_prepared_dims(const nk_prepared *p, int64_t dims[5]);
+/* Copies the prepared model and its maps (Prepared, src/internal.hpp:16-25);
+ * any pointer may be NULL.  scalars = {objective_scale, offset}. */
+nk_status nk_prepared_get(const nk_prepared *p, int64_t *ptr, int64_t *index, double *value,
+                          double *c, double *q, double *lb, double *ub, double *rl, double *ru,
+                          int64_t *cols, int64_t *rows, int64_t *lower_rows, int64_t *upper_rows,
+                          double *fixed, double *column_scale, double *row_scale, double *scalars,
+                          int64_t *qptr, int64_t *qindex, double *qvalue);
+
+/* Verifier::evaluate(x, y, safe_bound) -- src/verify.cpp:103-240, bit-identical.
+ * accuracy = {objective, primal, dual, gap, kkt, primal_absolute,
+ * dual_absolute, complementarity, lower_bound, finite}. */
+nk_status nk_verify(const nk_model *model, const double *x, const double *y, int safe_bound,
+                    double accuracy[10]);
+/* Verifier::infeasibility_bound(y) -- src/verify.cpp:93-101. */
+nk_status nk_infeasibility_bound(const nk_model *model, const double *y, double *bound);
+
+void nk_solve_defaults(nk_solve_options *options);
+/* Solves the model; x (n) and y (m) receive the returned primal and dual
+ * points (either may be NULL).  Errors (invalid model, CUDA failure, memory
+ * guard) return a status; termination outcomes are result->status. */
+nk_status nk_solve(const nk_model *model, const nk_solve_options *options,
+                   nk_solve_result *result, double *x, double *y);
+
 /* cuda_available / cuda_description / hardware_info --
  * include/vantage/vantage.hpp:76,145-146, src/cuda.cu:1267-1287. */
 int nk_cuda_available(void);

@@ -4,7 +4,9 @@
 
 The library is plain nvcc output (no torch extension machinery): C ABI only,
 CUDA runtime linked statically, FMA contraction disabled so the elementwise
-step formulas round exactly like the reference's CPU backend.
+step formulas round exactly like the reference's CPU backend.  The host C++
+(presolve, scaling, verifier) is compiled by g++ with OpenMP and without FMA
+contraction, the way the reference's host code is built.
 """
 from __future__ import annotations
 
@@ -19,6 +21,7 @@ ROOT = HERE.parent
 CSRC = HERE / "csrc"
 OUT = HERE / "libnkpdhg.so"
 SOURCES = ["nk_engine.cu"]
+HOST_SOURCES = ["nk_prepare.cpp"]  # plain C++: presolve, scaling, verifier
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -29,6 +32,15 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
+def gxx() -> str:
+    # the system g++ (its OpenMP runtime is installed); other toolchains on
+    # PATH may lack libgomp
+    for cand in ("/usr/bin/g++", shutil.which("g++")):
+        if cand and pathlib.Path(cand).exists():
+            return cand
+    raise RuntimeError("g++ not found")
+
+
 def _stale(out: pathlib.Path, deps) -> bool:
     if not out.exists():
         return True
@@ -37,7 +49,8 @@ def _stale(out: pathlib.Path, deps) -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> pathlib.Path:
-    deps = [CSRC / s for s in SOURCES] + list(CSRC.glob("*.cuh")) + [ROOT / "include" / "nk_pdhg.h"]
+    deps = ([CSRC / s for s in SOURCES + HOST_SOURCES] + list(CSRC.glob("*.cuh")) +
+            list(CSRC.glob("*.hpp")) + [ROOT / "include" / "nk_pdhg.h"])
     if not force and not _stale(OUT, deps):
         return OUT
     objs = []
@@ -52,8 +65,16 @@ def build(force: bool = False, verbose: bool = False) -> pathlib.Path:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.check_call(cmd)
         objs.append(str(obj))
+    for s in HOST_SOURCES:
+        obj = build_dir / (pathlib.Path(s).stem + ".o")
+        cmd = [gxx(), "-std=c++17", "-O2", "-fPIC", "-fopenmp", "-ffp-contract=off",
+               f"-I{ROOT / 'include'}", f"-I{CSRC}", "-c", str(CSRC / s), "-o", str(obj)]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.check_call(cmd)
+        objs.append(str(obj))
     tmp = OUT.with_suffix(".so.tmp")
-    cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs]
+    cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-Xcompiler", "-fopenmp", "-lgomp"]
     subprocess.check_call(cmd)
     tmp.replace(OUT)
     return OUT

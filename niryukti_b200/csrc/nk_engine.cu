@@ -9,11 +9,14 @@
 // and out, so callers only ever see their own order.
 #include "nk_common.cuh"
 #include "nk_device.cuh"
+#include "nk_host.hpp"
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 #include <algorithm>
+#include <chrono>
 #include <climits>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <numeric>
@@ -1199,6 +1202,62 @@ Engine *create_engine(const nk_csr *Ah, const nk_csr *Qh, const double *hc, cons
 
 } // namespace nk
 
+#include "nk_solve.cuh"
+
+namespace nk {
+// Copies a caller model (C ABI) into the host representation, after the
+// structural checks of Model::validate for the continuous part.
+HostModel host_model(const nk_model *model) {
+    if (!model)
+        throw Error(NK_ERR_INVALID, "null model");
+    const int64_t m = model->A.rows, n = model->A.cols;
+    if (m < 0 || n < 0 || !model->c || !model->lb || !model->ub || !model->rl || !model->ru)
+        throw Error(NK_ERR_INVALID, "incomplete model");
+    validate_csr(&model->A, m, n, "A");
+    const bool has_q = model->Q.rows > 0 && model->Q.ptr && model->Q.ptr[model->Q.rows] > 0;
+    if (has_q)
+        validate_csr(&model->Q, n, n, "Q");
+    HostModel hm;
+    auto csr = [](const nk_csr &c, Csr &out) {
+        out.rows = c.rows;
+        out.cols = c.cols;
+        out.ptr.assign(c.ptr, c.ptr + c.rows + 1);
+        out.index.assign(c.index, c.index + c.ptr[c.rows]);
+        out.value.assign(c.value, c.value + c.ptr[c.rows]);
+    };
+    csr(model->A, hm.A);
+    if (has_q)
+        csr(model->Q, hm.Q);
+    else {
+        hm.Q.rows = hm.Q.cols = n;
+        hm.Q.ptr.assign(size_t(n + 1), 0);
+    }
+    hm.c.assign(model->c, model->c + n);
+    hm.q = model->q ? std::vector<double>(model->q, model->q + n) : std::vector<double>(size_t(n), 0.0);
+    hm.lb.assign(model->lb, model->lb + n);
+    hm.ub.assign(model->ub, model->ub + n);
+    hm.rl.assign(model->rl, model->rl + m);
+    hm.ru.assign(model->ru, model->ru + m);
+    hm.offset = model->offset;
+    // the value checks of Model::validate (src/model.cpp:74-105)
+    if (!std::isfinite(hm.offset))
+        throw Error(NK_ERR_INVALID, "Invalid objective offset/sense");
+    for (size_t j = 0; j < size_t(n); ++j) {
+        if (!std::isfinite(hm.c[j]) || !std::isfinite(hm.q[j]))
+            throw Error(NK_ERR_INVALID, "Nonfinite objective coefficient");
+        const double l = hm.lb[j], u = hm.ub[j];
+        if (std::isnan(l) || std::isnan(u) || l == kInf || u == -kInf || l > u)
+            throw Error(NK_ERR_INVALID, "Invalid bounds for x" + std::to_string(j));
+    }
+    for (size_t i = 0; i < size_t(m); ++i) {
+        const double l = hm.rl[i], u = hm.ru[i];
+        if (std::isnan(l) || std::isnan(u) || l == kInf || u == -kInf || l > u)
+            throw Error(NK_ERR_INVALID, "Invalid row bounds");
+    }
+    return hm;
+}
+} // namespace nk
+
 using nk::guard;
 
 struct nk_pdhg {
@@ -1366,6 +1425,189 @@ nk_status nk_hardware_info(int *available, double *free_bytes, double *total_byt
             *free_bytes = double(f);
             *total_bytes = double(t);
         }
+    });
+}
+
+struct nk_prepared {
+    nk::Prepared p;
+};
+
+nk_status nk_prepare(const nk_model *model, int presolve, int scaling_combined, int scaling_passes,
+                     nk_prepared **out) {
+    return guard([&] {
+        if (!out)
+            throw nk::Error(NK_ERR_INVALID, "null output handle");
+        *out = nullptr;
+        if (scaling_passes < 0)
+            throw nk::Error(NK_ERR_INVALID, "negative scaling passes");
+        nk::HostModel hm = nk::host_model(model);
+        nk::PrepareOptions po;
+        po.presolve = presolve != 0;
+        po.scaling = scaling_combined ? "combined" : "ruiz";
+        po.scaling_passes = scaling_passes;
+        auto h = std::make_unique<nk_prepared>();
+        h->p = nk::prepare(hm, po);
+        *out = h.release();
+    });
+}
+void nk_prepared_free(nk_prepared *p) { delete p; }
+nk_status nk_prepared_dims(const nk_prepared *h, int64_t dims[5]) {
+    return guard([&] {
+        if (!h || !dims)
+            throw nk::Error(NK_ERR_INVALID, "null argument");
+        const auto &m = h->p.model;
+        dims[0] = int64_t(m.rl.size());
+        dims[1] = int64_t(m.c.size());
+        dims[2] = int64_t(m.A.value.size());
+        dims[3] = int64_t(m.Q.value.size());
+        dims[4] = h->p.failure.empty() ? 0 : 1;
+    });
+}
+nk_status nk_prepared_get(const nk_prepared *h, int64_t *ptr, int64_t *index, double *value,
+                          double *c, double *q, double *lb, double *ub, double *rl, double *ru,
+                          int64_t *cols, int64_t *rows, int64_t *lower_rows, int64_t *upper_rows,
+                          double *fixed, double *column_scale, double *row_scale, double *scalars,
+                          int64_t *qptr, int64_t *qindex, double *qvalue) {
+    return guard([&] {
+        if (!h)
+            throw nk::Error(NK_ERR_INVALID, "null handle");
+        const auto &p = h->p;
+        const auto &m = p.model;
+        auto put = [](auto *dst, const auto &v) {
+            if (dst && !v.empty())
+                std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+        };
+        put(ptr, m.A.ptr);
+        put(index, m.A.index);
+        put(value, m.A.value);
+        put(c, m.c);
+        put(q, m.q);
+        put(lb, m.lb);
+        put(ub, m.ub);
+        put(rl, m.rl);
+        put(ru, m.ru);
+        put(cols, p.cols);
+        put(rows, p.rows);
+        put(lower_rows, p.lower_rows);
+        put(upper_rows, p.upper_rows);
+        put(fixed, p.fixed);
+        put(column_scale, p.column_scale);
+        put(row_scale, p.row_scale);
+        if (scalars) {
+            scalars[0] = p.objective_scale;
+            scalars[1] = m.offset;
+        }
+        put(qptr, m.Q.ptr);
+        put(qindex, m.Q.index);
+        put(qvalue, m.Q.value);
+    });
+}
+nk_status nk_verify(const nk_model *model, const double *x, const double *y, int safe_bound,
+                    double accuracy[10]) {
+    return guard([&] {
+        if (!x || !y || !accuracy)
+            throw nk::Error(NK_ERR_INVALID, "null argument");
+        nk::HostModel hm = nk::host_model(model);
+        nk::Verifier v(hm);
+        auto a = v.evaluate(std::vector<double>(x, x + hm.c.size()),
+                            std::vector<double>(y, y + hm.rl.size()), safe_bound != 0);
+        const double s[10] = {a.objective,       a.primal,          a.dual,   a.gap,
+                              a.kkt,             a.primal_absolute, a.dual_absolute,
+                              a.complementarity, a.lower_bound,     a.finite ? 1.0 : 0.0};
+        std::memcpy(accuracy, s, sizeof(s));
+    });
+}
+nk_status nk_infeasibility_bound(const nk_model *model, const double *y, double *bound) {
+    return guard([&] {
+        if (!y || !bound)
+            throw nk::Error(NK_ERR_INVALID, "null argument");
+        nk::HostModel hm = nk::host_model(model);
+        *bound = nk::Verifier(hm).infeasibility_bound(std::vector<double>(y, y + hm.rl.size()));
+    });
+}
+
+void nk_solve_defaults(nk_solve_options *o) {
+    if (!o)
+        return;
+    *o = nk_solve_options{};
+    o->tol = 1e-6;
+    o->time_limit = 60;
+    o->iteration_limit = 100000;
+    o->check_every = 100;
+    o->presolve = 1;
+    o->scaling_passes = 5;
+    o->adaptive = 1;
+    o->restart = 1;
+    o->graphs = 1;
+    o->precision = NK_PRECISION_FP64;
+    o->refine = 1;
+}
+
+nk_status nk_solve(const nk_model *model, const nk_solve_options *o, nk_solve_result *result,
+                   double *x, double *y) {
+    return guard([&] {
+        if (!o || !result)
+            throw nk::Error(NK_ERR_INVALID, "null argument");
+        nk::HostModel hm = nk::host_model(model);
+        const int64_t m = model->A.rows, n = model->A.cols;
+        if (!(o->tol > 0) || o->check_every <= 0 || o->iteration_limit < 0 || !(o->time_limit >= 0) ||
+            o->scaling_passes < 0 || o->precision < 0 || o->precision > 2)
+            throw nk::Error(NK_ERR_INVALID, "invalid solve options");
+        nk::SolveSettings S;
+        S.driver.tol = o->tol;
+        S.driver.time_limit = o->time_limit;
+        S.driver.iteration_limit = o->iteration_limit;
+        S.driver.check_every = o->check_every;
+        S.driver.adaptive = o->adaptive != 0;
+        S.driver.restart = o->restart != 0;
+        S.driver.graphs = o->graphs != 0;
+        S.driver.index_bits = o->index_bits;
+        S.driver.verbose = o->verbose != 0;
+        S.prepare.presolve = o->presolve != 0;
+        S.prepare.scaling = o->scaling_combined ? "combined" : "ruiz";
+        S.prepare.scaling_passes = o->scaling_passes;
+        S.precision = o->precision;
+        S.refine = o->refine != 0;
+        S.phase_tol = o->phase_tol;
+        if (o->initial_x)
+            S.initial_x.assign(o->initial_x, o->initial_x + n);
+        if (o->initial_y)
+            S.initial_y.assign(o->initial_y, o->initial_y + m);
+        nk::SolveReport R = nk::solve(hm, S);
+        nk_solve_result &r = *result;
+        r = nk_solve_result{};
+        r.status = R.status;
+        r.iterations = R.iterations;
+        r.restarts = R.restarts;
+        r.rejected_steps = R.rejected;
+        r.weight_updates = R.weight_updates;
+        r.device_checks = R.device_checks;
+        r.host_checks = R.host_checks;
+        r.removed_rows = R.removed_rows;
+        r.removed_columns = R.removed_columns;
+        r.phase_iterations = R.mixed_iterations;
+        r.refine_iterations = R.refine_iterations;
+        r.seconds = R.seconds;
+        r.preprocess_seconds = R.preprocess;
+        r.transfer_seconds = R.transfer;
+        r.iteration_seconds = R.iteration;
+        r.verification_seconds = R.verification;
+        r.phase_seconds = R.mixed_seconds;
+        r.objective = R.accuracy.objective;
+        r.kkt = R.accuracy.kkt;
+        r.primal = R.accuracy.primal;
+        r.dual = R.accuracy.dual;
+        r.gap = R.accuracy.gap;
+        r.lower_bound = R.accuracy.lower_bound;
+        r.phase_objective = R.mixed.objective;
+        r.phase_kkt = R.mixed.kkt;
+        r.phase_primal = R.mixed.primal;
+        r.phase_dual = R.mixed.dual;
+        r.phase_gap = R.mixed.gap;
+        if (x && R.x.size() == size_t(n))
+            std::memcpy(x, R.x.data(), size_t(n) * 8);
+        if (y && R.y.size() == size_t(m))
+            std::memcpy(y, R.y.data(), size_t(m) * 8);
     });
 }
 }

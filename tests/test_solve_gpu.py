@@ -1,0 +1,126 @@
+"""Device-resident solve (nk_solve) against the oracle and the reference.
+
+Termination is certified by the host verifier (bit-identical to the
+reference's, tests/test_host.py), so an OPTIMAL result here is a point whose
+outward-rounded relative KKT error is <= tol on the caller's model.  Each test
+also compares the objective with the CPU oracle (or the reference build where
+the model needs presolve): both are 1e-6-KKT points, so their objectives agree
+to the tolerance the relative gap implies, |f1 - f2| <= 2 tol (1 + |f|).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from niryukti_b200 import synth
+from tests.test_host import infeasible_models, presolve_model
+from tests.test_oracle import sparse_qp_model, tiny
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-6
+
+
+def objective_close(a, b, tol=TOL):
+    assert abs(a - b) <= 2 * tol * (1 + abs(b)), (a, b)
+
+
+@pytest.fixture(scope="module")
+def solver(gpu):
+    from niryukti_b200 import solver as s
+    return s
+
+
+def test_solve_config1_lp(solver, oracle):
+    model = synth.random_lp(m=2000, n=5000, per_col=5, seed=1)
+    r = solver.solve(model, tol=TOL)
+    assert r["status"] == "OPTIMAL", r
+    assert r["kkt"] <= TOL
+    again = solver.verify(model, r["x"], r["y"])  # certified independently of the solve
+    assert again["kkt"] <= TOL
+    ref = oracle.model(model).solve(tol=TOL)
+    assert ref["status"] == "OPTIMAL"
+    objective_close(r["objective"], ref["objective"])
+    assert r["device_checks"] >= r["iterations"] // 100 - 1
+    assert r["host_checks"] <= 3  # certification only, not every check
+
+
+def test_solve_known_answers(solver):
+    r = solver.solve(sparse_qp_model())  # tests/test_research.cpp:118-125
+    assert r["status"] == "OPTIMAL"
+    assert abs(r["objective"] + 7) < 1e-5 and np.allclose(r["x"], [1, 2], atol=1e-4)
+    m = tiny(2, 2, [(0, 0, 1.0), (0, 1, 1.0), (1, 0, 1.0), (1, 1, -1.0)])
+    m.lb[:] = 0
+    m.ub[:] = 4
+    m.c = np.array([1.0, 2.0])
+    m.rl = np.array([2.0, -1.0])
+    m.ru = np.array([3.0, 2.0])
+    r = solver.solve(m, iteration_limit=200000)
+    assert r["status"] == "OPTIMAL"
+    assert abs(r["objective"] - 2) < 1e-5
+
+
+def test_solve_with_presolve_reductions(solver, reference):
+    model = presolve_model()
+    r = solver.solve(model)
+    ref = reference.model(model).solve(method="pdhg", device="cpu")
+    assert r["status"] == ref["status"] == "OPTIMAL", (r["status"], ref["status"])
+    assert r["removed_rows"] == ref["removed_rows"] and r["removed_columns"] == ref["removed_columns"]
+    objective_close(r["objective"], ref["objective"])
+
+
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_reduced_precision_then_fp64_refinement(solver, oracle, precision):
+    model = synth.random_lp(m=2000, n=5000, per_col=5, seed=1)
+    r = solver.solve(model, matrix_precision=precision, refine=True)
+    assert r["status"] == "OPTIMAL", r
+    assert r["kkt"] <= TOL
+    assert r["phase_iterations"] > 0 and math.isfinite(r["phase_kkt"])
+    ref = oracle.model(model).solve(tol=TOL)
+    objective_close(r["objective"], ref["objective"])
+
+
+def test_reduced_precision_without_refinement(solver, oracle):
+    """FP32 matrices alone: the certified accuracy it reaches is reported, and
+    with a looser stated tolerance it terminates OPTIMAL."""
+    model = synth.random_lp(m=2000, n=5000, per_col=5, seed=1)
+    r = solver.solve(model, matrix_precision="fp32", refine=False, tol=1e-4)
+    assert r["status"] == "OPTIMAL", r
+    assert r["kkt"] <= 1e-4
+    ref = oracle.model(model).solve(tol=TOL)
+    objective_close(r["objective"], ref["objective"], 1e-4)
+
+
+def test_presolve_infeasible(solver):
+    for name, model in infeasible_models().items():
+        assert solver.solve(model)["status"] == "INFEASIBLE", name
+
+
+def test_infeasible_certificate_from_iterates(solver, reference):
+    # x0 + x1 >= 3 and 2 x0 + 2 x1 <= 2: no presolve rule applies, the Farkas
+    # ray comes from the iterates (src/solver.cpp:599-633)
+    from tests.test_host import from_rows
+    model = from_rows(2, [[(0, 1.0), (1, 1.0)], [(0, 2.0), (1, 2.0)]], c=[1.0, 1.0],
+                      lb=[0, 0], ub=[5, 5], rl=[3, -math.inf], ru=[math.inf, 2])
+    r = solver.solve(model)
+    assert r["status"] == "INFEASIBLE"
+    assert reference.model(model).infeasibility_bound(r["y"]) > 0
+    assert reference.model(model).solve(method="pdhg", device="cpu")["status"] == "INFEASIBLE"
+
+
+def test_limits(solver):
+    model = synth.random_lp(m=2000, n=5000, per_col=5, seed=1)
+    r = solver.solve(model, iteration_limit=300)
+    assert r["status"] == "ITERATION_LIMIT" and r["iterations"] <= 300
+    assert r["kkt"] > TOL and math.isfinite(r["kkt"])  # best point, certified
+    r = solver.solve(model, time_limit=0)
+    assert r["status"] == "TIME_LIMIT"
+
+
+def test_power_law_lp_solves(solver, oracle):
+    model = synth.power_law_lp(m=20000, n=40000, nnz=400000, seed=7)
+    r = solver.solve(model, time_limit=120)
+    assert r["status"] == "OPTIMAL", {k: r[k] for k in ("status", "iterations", "kkt")}
+    ref = oracle.model(model).solve(tol=TOL, time_limit=300)
+    if ref["status"] == "OPTIMAL":
+        objective_close(r["objective"], ref["objective"])
