@@ -222,6 +222,88 @@ def reference_arm(args, world, rank):
     print(json.dumps(line))
 
 
+# ---------------------------------------------------------------- solves
+def solve_models(args):
+    from niryukti_b200 import synth
+    c1 = synth.random_lp(m=2000, n=5000, per_col=5, seed=1)
+    c2 = build_model(args)
+    return {"config1_lp_m2000_n5000": c1, "config2_power_law_lp" + ("_small" if args.small else
+                                                                     "_m1e6_n2e6_nnz2e7"): c2}
+
+
+def reference_solve(model, budget, threads):
+    """The reference's own solve (vantage::solve, method pdhg, device cpu) from
+    oracle/_ref, with its per-check verbose lines turned into times to each KKT
+    decade; None when the reference build is absent."""
+    from oracle import oracle as orc
+    if not orc.REF_SO.exists():
+        return None
+    import re
+    r, text = None, ""
+    fd, path = tempfile.mkstemp(suffix=".log")
+    saved = os.dup(2)
+    try:
+        os.dup2(fd, 2)  # the reference prints its check lines on stderr
+        r = orc.Reference().model(model).solve(method="pdhg", device="cpu", verbose=True,
+                                               time_limit=budget, threads=threads,
+                                               iteration_limit=10**9)
+    finally:
+        os.dup2(saved, 2)
+        os.close(saved)
+        os.close(fd)
+        text = pathlib.Path(path).read_text()
+        os.unlink(path)
+    reached, best = {}, math.inf
+    for mt in re.finditer(r"iter=(\d+).*?primal=(\S+) dual=(\S+) gap=(\S+) seconds=(\S+)", text):
+        kkt = max(float(mt.group(2)), float(mt.group(3)), float(mt.group(4)))
+        best = min(best, kkt)
+        for k in range(9):
+            if best <= 10.0 ** -k and f"1e-{k}" not in reached:
+                reached[f"1e-{k}"] = float(mt.group(5))
+    return {"status": r["status"], "seconds": r["seconds"], "iterations": r["iterations"],
+            "kkt": r["kkt"], "objective": r["objective"], "time_to_kkt": reached,
+            "preprocess_seconds": r["preprocess_seconds"], "threads": threads}
+
+
+def solve_child(args):
+    out = {}
+    for name, model in solve_models(args).items():
+        budget = args.cpu_solve_seconds if "config2" in name else 300.0
+        out[name] = reference_solve(model, budget, args.cpu_threads)
+    print(json.dumps(out))
+
+
+def solve_section(args):
+    """Time to 1e-6 relative KKT through the public solve API (host model in,
+    certified x, y out): config 1 to tolerance, config 2 within a budget, each
+    beside the reference's own CPU solve of the same LP."""
+    from niryukti_b200 import solver
+    res = {}
+    for name, model in solve_models(args).items():
+        budget = args.solve_seconds if "config2" in name else 300.0
+        r = solver.solve(model, tol=1e-6, time_limit=budget, iteration_limit=10**9,
+                         matrix_precision="fp64")
+        res[name] = {"gpu": {k: r[k] for k in (
+            "status", "seconds", "iterations", "kkt", "primal", "dual", "gap", "objective",
+            "restarts", "preprocess_seconds", "transfer_seconds", "iteration_seconds",
+            "verification_seconds", "device_checks", "host_checks", "time_to_kkt")}}
+        res[name]["gpu"]["budget_s"] = budget
+    if not args.no_cpu:
+        cmd = [sys.executable, str(pathlib.Path(__file__).resolve()), "--solve-child",
+               "--cpu-threads", str(args.cpu_threads), "--cpu-solve-seconds",
+               str(args.cpu_solve_seconds)] + (["--small"] if args.small else [])
+        env = dict(os.environ, OMP_NUM_THREADS=str(args.cpu_threads))
+        try:
+            out = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=1800)
+            cpu = json.loads(out.stdout.strip().splitlines()[-1])
+            for name in res:
+                res[name]["reference_cpu"] = cpu.get(name)
+        except Exception as exc:
+            for name in res:
+                res[name]["reference_cpu"] = {"error": str(exc)[-300:]}
+    return res
+
+
 # ---------------------------------------------------------------- engine arm
 def engine_arm(args, world, rank, local):
     import torch
@@ -348,6 +430,9 @@ def engine_arm(args, world, rank, local):
                     "path": "nk_pdhg_reset + nk_pdhg_advance(100) + nk_pdhg_candidates"},
             "gpu_launches": 2 * (args.steps * TRIALS_PER_STEP),
             "clocks": clocks.summary(), "accepted_trials": accepted}
+    del g
+    if not args.no_solve:
+        line["solve"] = solve_section(args)
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
@@ -369,13 +454,21 @@ def main():
     ap.add_argument("--ref-trials", type=int, default=10)
     ap.add_argument("--profile-trials", type=int, default=20)
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-solve", action="store_true", help="skip the time-to-tolerance solves")
+    ap.add_argument("--solve-seconds", type=float, default=60.0,
+                    help="time budget of the config-2 solve on the GPU")
+    ap.add_argument("--cpu-solve-seconds", type=float, default=30.0,
+                    help="time budget of the reference's config-2 CPU solve")
+    ap.add_argument("--solve-child", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per launch of the top kernel from an ncu capture")
     args = ap.parse_args()
-    if args.warmup < 3 and not args.cpu_child:
+    if args.warmup < 3 and not (args.cpu_child or args.solve_child):
         ap.error("--warmup must be at least 3")
     if args.cpu_child:
         return cpu_child(args)
+    if args.solve_child:
+        return solve_child(args)
     world, rank, local = dist_setup()
     if args.impl == "reference":
         return reference_arm(args, world, rank)

@@ -191,6 +191,9 @@ typedef struct {
     double objective, kkt, primal, dual, gap, lower_bound;
     /* accuracy of the reduced-precision phase's best point (no safe bound) */
     double phase_objective, phase_kkt, phase_primal, phase_dual, phase_gap;
+    /* seconds from the call until the device estimate of the best candidate's
+     * relative KKT error first fell to 10^-k (k = 0..8); -1: never */
+    double reached[9];
 } nk_solve_result;
 
 /* prepare(model, options) -- src/preprocess.cpp:133-346: presolve (fixed and

@@ -13,6 +13,7 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <climits>
 #include <cmath>
@@ -1604,6 +1605,8 @@ nk_status nk_solve(const nk_model *model, const nk_solve_options *o, nk_solve_re
         r.phase_primal = R.mixed.primal;
         r.phase_dual = R.mixed.dual;
         r.phase_gap = R.mixed.gap;
+        for (int k = 0; k < 9; ++k)
+            r.reached[k] = R.reached[k];
         if (x && R.x.size() == size_t(n))
             std::memcpy(x, R.x.data(), size_t(n) * 8);
         if (y && R.y.size() == size_t(m))

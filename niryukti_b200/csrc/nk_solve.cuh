@@ -197,6 +197,55 @@ __global__ void __launch_bounds__(kThreads) displacement_partial(int64_t n, int6
     }
 }
 
+// Farkas screen of a candidate ray r = y - ey (ey may be null) with
+// A^T r = aty - atey (atey may be null), prepared space.  The caller-space ray
+// is a positive row scaling of r, so signs carry over.  Values: 0 the ray is
+// impossible (max) -- a sign meets an infinite caller row bound, or A^T r
+// pushes a column towards an infinite bound, where the outward-rounded
+// feasibility bound (lp_lower_bound, src/verify.cpp:12-88) is -infinity;
+// 1 + 2 that bound in plain FP64 (-sum r_i b_i + sum_j min over the box of
+// (A^T r)_j x_j); 3 the magnitude of its terms.
+constexpr int kRayValues = 4;
+__global__ void __launch_bounds__(kThreads) ray_screen(int64_t n, int64_t m, const double *y,
+                                                       const double *ey, const double *aty,
+                                                       const double *atey, KktArgs a,
+                                                       double *part) {
+    __shared__ double smem[kWarps * kRayValues];
+    double v[kRayValues] = {0, 0, 0, 0};
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    const int64_t top = n > m ? n : m;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < top; i += stride) {
+        if (i < m) {
+            const double r = (y[i] - (ey ? ey[i] : 0.)) * a.rs[i] * a.os;
+            if (r != 0) {
+                const double b = r > 0 ? a.oru[i] : a.orl[i];
+                if (!isfinite(b))
+                    v[0] = 1;
+                else {
+                    v[1] -= r * b;
+                    v[3] += fabs(r * b);
+                }
+            }
+        }
+        if (i < n) {
+            const double g = (aty[i] - (atey ? atey[i] : 0.)) * a.os / a.cs[i];
+            if (g != 0) {
+                const double b = g > 0 ? a.olb[i] : a.oub[i];
+                if (!isfinite(b))
+                    v[0] = 1;
+                else {
+                    v[2] += g * b;
+                    v[3] += fabs(g * b);
+                }
+            }
+        }
+    }
+    block_combine<kRayValues>(v, 1u, smem);
+    if (threadIdx.x == 0)
+        for (int t = 0; t < kRayValues; ++t)
+            part[blockIdx.x * kRayValues + t] = v[t];
+}
+
 // ------------------------------------------------------------------ driver
 struct SolveReport {
     int status = NK_SOLVE_ITERATION_LIMIT;
@@ -207,6 +256,7 @@ struct SolveReport {
     Accuracy accuracy, mixed;
     int64_t mixed_iterations = 0;
     double mixed_seconds = 0;
+    double reached[9] = {-1, -1, -1, -1, -1, -1, -1, -1, -1}; // seconds to best kkt <= 10^-k
     std::vector<double> x, y;
 };
 
@@ -222,8 +272,9 @@ struct DeviceSolve {
     std::unique_ptr<Engine> E;
     int64_t n = 0, m = 0;
     DevBuf<double> cs, olb, oub, rs, shift, orl, oru;       // KKT constants, engine order
-    DevBuf<double> k_ax, k_aty, k_qx, best_x, best_y, epoch_x, epoch_y, part, out;
-    double *host_out = nullptr; // pinned: 2 candidates x kKktValues, then 2 displacement sums
+    DevBuf<double> k_ax, k_aty[2], k_qx, best_x, best_y, epoch_x, epoch_y, epoch_aty, part, out;
+    double *host_out = nullptr; // pinned: 2 candidates x kKktValues, 2 displacement sums,
+                                // 3 rays x kRayValues
     int grid = 148;
     double os = 1, cscale = 1, offset_o = 0, offset_s = 0, cfixed = 0;
     std::vector<int64_t> cperm, rperm; // engine position -> prepared index
@@ -310,7 +361,9 @@ struct DeviceSolve {
         }
         auto vec = [&](DevBuf<double> &d, int64_t len) { d.alloc(size_t(std::max<int64_t>(1, len))); };
         vec(k_ax, m);
-        vec(k_aty, n);
+        vec(k_aty[0], n);
+        vec(k_aty[1], n);
+        vec(epoch_aty, n);
         vec(k_qx, n);
         vec(best_x, n);
         vec(best_y, m);
@@ -320,18 +373,27 @@ struct DeviceSolve {
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         grid = int(std::max<int64_t>(1, std::min<int64_t>(int64_t(sms) * 4, (std::max(n, m) + kThreads - 1) / kThreads)));
-        part.alloc(size_t(grid) * kKktValues);
-        out.alloc(2 * kKktValues + 2);
-        cuda_check(cudaMallocHost(reinterpret_cast<void **>(&host_out), (2 * kKktValues + 2) * sizeof(double)),
+        part.alloc(size_t(grid) * std::max(kKktValues, kRayValues));
+        out.alloc(kOutValues);
+        cuda_check(cudaMallocHost(reinterpret_cast<void **>(&host_out), kOutValues * sizeof(double)),
                    "pinned");
         int cur = current();
-        copy(epoch_x.p, E->x[cur].p, n);
-        copy(epoch_y.p, E->y[cur].p, m);
         copy(best_x.p, E->x[cur].p, n);
         copy(best_y.p, E->y[cur].p, m);
+        set_epoch(cur);
         cuda_check(cudaStreamSynchronize(s), "driver setup");
     }
 
+    static constexpr int kOutValues = 2 * kKktValues + 2 + 3 * kRayValues;
+    static constexpr int kRayOut = 2 * kKktValues + 2;
+
+    // epoch = current iterate (after a restart), with its A^T epoch_y
+    void set_epoch(int cur) {
+        copy(epoch_x.p, E->x[cur].p, n);
+        copy(epoch_y.p, E->y[cur].p, m);
+        if (n)
+            E->spmv(E->At, epoch_y.p, epoch_aty.p);
+    }
     void copy(double *dst, const double *src, int64_t len) {
         if (len)
             cuda_check(cudaMemcpyAsync(dst, src, size_t(len) * 8, cudaMemcpyDeviceToDevice, E->stream),
@@ -347,16 +409,20 @@ struct DeviceSolve {
     // Launches the evaluation of the prepared point (x, y) into out[slot]; the
     // products A x, A^T y (and Q x) are recomputed, not taken from the
     // engine's incrementally updated activity.
+    KktArgs args(const double *x, const double *y, int slot) {
+        return KktArgs{n, m, x, y, k_ax.p, k_aty[slot].p, E->sparse_q ? k_qx.p : nullptr, E->c.p,
+                       E->q.p, cs.p, olb.p, oub.p, rs.p, shift.p, orl.p, oru.p, os, cscale,
+                       E->sparse_q ? 1 : 0};
+    }
     void evaluate(const double *x, const double *y, int slot) {
         cudaStream_t s = E->stream;
         if (m)
             E->spmv(E->A, x, k_ax.p);
         if (n)
-            E->spmv(E->At, y, k_aty.p);
+            E->spmv(E->At, y, k_aty[slot].p);
         if (E->sparse_q)
             E->q_spmv(x, k_qx.p);
-        KktArgs a{n, m, x, y, k_ax.p, k_aty.p, E->sparse_q ? k_qx.p : nullptr, E->c.p, E->q.p,
-                  cs.p, olb.p, oub.p, rs.p, shift.p, orl.p, oru.p, os, cscale, E->sparse_q ? 1 : 0};
+        KktArgs a = args(x, y, slot);
         kkt_partial<<<grid, kThreads, 0, s>>>(a, part.p);
         finish_partials<kKktValues><<<1, kThreads, 0, s>>>(part.p, grid, kKktMaxMask,
                                                           out.p + slot * kKktValues);
@@ -367,6 +433,35 @@ struct DeviceSolve {
         displacement_partial<<<grid, kThreads, 0, s>>>(n, m, x, epoch_x.p, y, epoch_y.p, part.p);
         finish_partials<2><<<1, kThreads, 0, s>>>(part.p, grid, 0u, out.p + 2 * kKktValues);
         cuda_check(cudaGetLastError(), "displacement");
+    }
+    // Screens the three candidate rays of the infeasibility test on the device:
+    // ray 0 the chosen candidate's y (slot `chosen`), ray 1 the other one's,
+    // ray 2 the chosen y minus the epoch y.  Returns, per ray, whether the
+    // outward-rounded host bound could still be positive.
+    std::array<bool, 3> screen_rays(const double *y_chosen, int chosen, const double *y_other) {
+        cudaStream_t s = E->stream;
+        const double *ys[3] = {y_chosen, y_other, y_chosen};
+        const double *eys[3] = {nullptr, nullptr, epoch_y.p};
+        const double *atys[3] = {k_aty[chosen].p, k_aty[1 - chosen].p, k_aty[chosen].p};
+        const double *ateys[3] = {nullptr, nullptr, epoch_aty.p};
+        KktArgs a = args(nullptr, nullptr, 0);
+        for (int r = 0; r < 3; ++r) {
+            ray_screen<<<grid, kThreads, 0, s>>>(n, m, ys[r], eys[r], atys[r], ateys[r], a, part.p);
+            finish_partials<kRayValues><<<1, kThreads, 0, s>>>(part.p, grid, 1u,
+                                                               out.p + kRayOut + r * kRayValues);
+        }
+        cuda_check(cudaGetLastError(), "ray screen");
+        cuda_check(cudaMemcpyAsync(host_out + kRayOut, out.p + kRayOut, 3 * kRayValues * 8,
+                                   cudaMemcpyDeviceToHost, s), "ray screen");
+        cuda_check(cudaStreamSynchronize(s), "ray screen");
+        std::array<bool, 3> ok{};
+        for (int r = 0; r < 3; ++r) {
+            const double *v = host_out + kRayOut + r * kRayValues;
+            // FP64 sums of the bound's terms err by far less than 1e-9 of their
+            // magnitude: below that margin the exact bound is negative too
+            ok[size_t(r)] = v[0] == 0 && v[1] + v[2] > -1e-9 * (1 + v[3]);
+        }
+        return ok;
     }
     void fetch(int values) {
         cuda_check(cudaMemcpyAsync(host_out, out.p, size_t(values) * 8, cudaMemcpyDeviceToHost, E->stream),
@@ -496,6 +591,10 @@ struct Driver {
                 D.copy(D.best_x.p, cx, n);
                 D.copy(D.best_y.p, cy, m);
                 best = ca;
+                double level = 1;
+                for (int k = 0; k < 9; ++k, level /= 10)
+                    if (best.kkt <= level && R.reached[k] < 0)
+                        R.reached[k] = since(start);
             }
             R.verification += since(tick);
             if (o.verbose)
@@ -526,10 +625,15 @@ struct Driver {
                     next_host_check = R.iterations + std::max<int64_t>(1000, 10 * o.check_every);
                 }
             }
-            // infeasibility certificates (src/solver.cpp:599-633), every 10th check
-            if (certify && R.iterations >= 1000 && ca.primal > o.tol && checks % 10 == 0) {
+            // infeasibility certificates (src/solver.cpp:599-633): the rays the
+            // device screen cannot rule out go to the outward-rounded host test
+            if (certify && R.iterations >= 1000 && ca.primal > o.tol) {
                 tick = SteadyClock::now();
-                if (infeasible(cy))
+                const double *other_y = avg ? E.y[cur].p : E.ya.p;
+                auto ok = D.screen_rays(cy, avg ? 1 : 0, other_y);
+                if ((ok[0] || ok[1] || ok[2]) &&
+                    infeasible(ok[0] ? cy : nullptr, ok[1] ? other_y : nullptr,
+                               ok[2] ? cy : nullptr))
                     return true;
                 R.verification += since(tick);
             }
@@ -558,9 +662,7 @@ struct Driver {
                     }
                 }
                 E.reset_candidate(avg);
-                int now = D.current();
-                D.copy(D.epoch_x.p, E.x[now].p, n);
-                D.copy(D.epoch_y.p, E.y[now].p, m);
+                D.set_epoch(D.current());
                 restart_kkt = ca.kkt;
                 since_restart = 0;
                 R.restarts++;
@@ -569,20 +671,25 @@ struct Driver {
         return false;
     }
 
-    // Rays from the current/averaged dual and the epoch displacement, scaled to
-    // unit max norm and certified by the outward-rounded Farkas bound.
-    bool infeasible(const double *cy_dev) {
-        Engine &E = *D.E;
-        int cur = D.current();
-        auto y_cur = D.download_rows(E.y[cur].p);
-        auto y_avg = D.download_rows(E.ya.p);
-        auto y_dis = D.download_rows(cy_dev);
-        auto y_epo = D.download_rows(D.epoch_y.p);
-        for (size_t i = 0; i < y_dis.size(); ++i)
-            y_dis[i] -= y_epo[i];
+    // Rays from the chosen and the other candidate's dual and from the chosen
+    // dual's displacement since the last restart, scaled to unit max norm and
+    // certified by the outward-rounded Farkas bound; null: ruled out on the device.
+    bool infeasible(const double *chosen, const double *other, const double *displaced) {
+        std::vector<std::vector<double>> rays;
+        if (chosen)
+            rays.push_back(D.download_rows(chosen));
+        if (other)
+            rays.push_back(D.download_rows(other));
+        if (displaced) {
+            auto y = D.download_rows(displaced);
+            auto e = D.download_rows(D.epoch_y.p);
+            for (size_t i = 0; i < y.size(); ++i)
+                y[i] -= e[i];
+            rays.push_back(std::move(y));
+        }
         R.host_checks++;
-        for (auto *src : {&y_cur, &y_avg, &y_dis}) {
-            auto ray = D.prep.restore_y(*src, D.orig.rl.size());
+        for (auto &src : rays) {
+            auto ray = D.prep.restore_y(src, D.orig.rl.size());
             double norm = 0;
             bool finite = true;
             for (double v : ray) {

@@ -47,7 +47,8 @@ class NkSolveResult(C.Structure):
                     "seconds", "preprocess_seconds", "transfer_seconds", "iteration_seconds",
                     "verification_seconds", "phase_seconds", "objective", "kkt", "primal",
                     "dual", "gap", "lower_bound", "phase_objective", "phase_kkt",
-                    "phase_primal", "phase_dual", "phase_gap")]]
+                    "phase_primal", "phase_dual", "phase_gap")],
+                ("reached", C.c_double * 9)]
 
 
 def _bind():
@@ -145,8 +146,10 @@ def solve(model, *, tol=1e-6, time_limit=60.0, iteration_limit=100000, check_eve
     r = NkSolveResult()
     check(L.nk_solve(C.byref(view.s), C.byref(o), C.byref(r), x.ctypes.data_as(_D),
                      y.ctypes.data_as(_D)))
-    out = {k: getattr(r, k) for k, _ in NkSolveResult._fields_}
+    out = {k: getattr(r, k) for k, _ in NkSolveResult._fields_ if k != "reached"}
     out["status"] = STATUS[r.status]
+    # seconds until the best candidate's KKT error first reached 10^-k
+    out["time_to_kkt"] = {f"1e-{k}": r.reached[k] for k in range(9) if r.reached[k] >= 0}
     out["kkt_error"] = r.kkt
     out["primal_residual"], out["dual_residual"], out["relative_gap"] = r.primal, r.dual, r.gap
     out["total_seconds"] = r.seconds
