@@ -1,0 +1,62 @@
+"""The drop-in: the reference's own host code with the B200 engine at its
+cuda_backend() seam (oracle/_ref/libvantage_nk.so, built by `make -C oracle
+bridge` from the reference sources plus niryukti_b200/bridge/).
+
+Everything above the seam is the reference's unmodified code: its backend
+factory, its solve_continuous driver, presolve and verifier.  The tests check
+that the bridged CUDA backend steps like the reference's CPU backend and that
+the reference's own solve with --device cuda reaches its CPU answer.
+"""
+import json
+
+import numpy as np
+import pytest
+
+from niryukti_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def bridged(gpu):
+    from oracle.oracle import BRIDGE_SO, Reference
+    if not BRIDGE_SO.exists():
+        pytest.fail("bridged reference build oracle/_ref/libvantage_nk.so is missing")
+    return Reference(BRIDGE_SO)
+
+
+def test_bridge_reports_the_device(bridged):
+    assert bridged.cuda_available()
+
+
+@pytest.mark.parametrize("kw", [dict(adaptive=False), dict(halpern=True, reflection=1.0)])
+def test_bridged_backend_steps_like_cpu(bridged, reference, kw):
+    model = synth.random_lp(m=300, n=700, per_col=4, seed=3)
+    x0, y0 = np.zeros(model.n), np.zeros(model.m)
+    tau = sigma = 0.05
+    cpu = reference.model(model).backend(x0, y0, device="cpu", **kw)
+    gpu = bridged.model(model).backend(x0, y0, device="cuda", graphs=True, **kw)
+    for _ in range(3):  # fixed steps: every trial is accepted on both sides
+        assert gpu.advance(50, tau, sigma) == cpu.advance(50, tau, sigma)
+        for a, b in zip(gpu.candidates(), cpu.candidates()):
+            assert np.allclose(a, b, rtol=1e-11, atol=1e-11)
+
+
+def test_bridged_solve_matches_cpu_solve(bridged, reference):
+    from tests.conftest import load_golden
+    model, d = load_golden("solve_small_lp")
+    want = json.loads(str(d["result"]))
+    r = bridged.model(model).solve(method="pdhg", device="cuda", iteration_limit=200000)
+    assert r["status"] == want["status"] == "OPTIMAL"
+    assert r["kkt"] <= 1e-6
+    assert abs(r["objective"] - want["objective"]) <= 2e-6 * (1 + abs(want["objective"]))
+
+
+def test_bridged_solve_mixed_precision(bridged):
+    from tests.conftest import load_golden
+    model, d = load_golden("solve_small_lp")
+    want = json.loads(str(d["result"]))
+    r = bridged.model(model).solve(method="pdhg", device="cuda", matrix_precision="mixed",
+                                   cuda_graphs=True, iteration_limit=200000)
+    assert r["status"] == "OPTIMAL" and r["kkt"] <= 1e-6
+    assert abs(r["objective"] - want["objective"]) <= 2e-6 * (1 + abs(want["objective"]))
