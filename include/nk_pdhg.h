@@ -230,6 +230,35 @@ nk_status nk_solve(const nk_model *model, const nk_solve_options *options,
 
 /* cuda_available / cuda_description / hardware_info --
  * include/vantage/vantage.hpp:76,145-146, src/cuda.cu:1267-1287. */
+/* KKT proxy without any device allocation.  No counterpart in the reference:
+ * it exists for callers that must not allocate device memory themselves --
+ * a host application that hands all device memory to its own pool or budget
+ * (a solve service admitting work by memory footprint), or a latency-critical
+ * loop in which cudaMalloc / cudaFree would synchronise the device.
+ *
+ * Computes the same scaled KKT proxy as one point of nk_pdhg_monitor (the
+ * monitor kernel of src/cuda.cu:387-446) for caller-provided DEVICE vectors:
+ * x, c, q, lb, ub, aty (= A^T y) and qx (= Q x, or NULL) of length n; y, ax
+ * (= A x), rl, ru of length m; cscale = max(1, 1 + max |c_j|).  The result
+ * (one double) is written to the DEVICE pointer `result` on `stream`
+ * (a cudaStream_t; NULL = the default stream); nothing is synchronised.
+ *
+ * The kernel's per-block partial sums and its arrival counter live in one
+ * fixed array in the library (about 640 KiB, held on every GPU that loads the
+ * library until the process exits), so n and m are limited to
+ * NK_MONITOR_STATIC_MAX entries each; larger inputs fail with NK_ERR_INVALID.
+ * The first call on each device looks up that array's device address (and
+ * may load the module), so make it before any stream capture.  All calls share
+ * the array: the counter is cleared on `stream` before every launch, and calls
+ * whose kernels can overlap on the GPU (different streams, or different host
+ * threads) race and must be serialised by the caller. */
+#define NK_MONITOR_STATIC_MAX 4194304
+nk_status nk_monitor_static(int64_t n, int64_t m, const double *x, const double *y,
+                            const double *ax, const double *aty, const double *qx,
+                            const double *c, const double *q, const double *lb, const double *ub,
+                            const double *rl, const double *ru, double cscale, double *result,
+                            void *stream);
+
 int nk_cuda_available(void);
 nk_status nk_cuda_description(char *buffer, int length);
 nk_status nk_hardware_info(int *available, double *free_bytes, double *total_bytes);

@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <vector>
 
@@ -1316,6 +1317,69 @@ nk_status nk_pdhg_monitor(nk_pdhg *h, double *out) {
         *out = h->e->monitor();
     });
 }
+// ---- KKT proxy on fixed library scratch (see nk_monitor_static in nk_pdhg.h).
+// Callers that may not allocate device memory get the monitor kernel launched
+// on this array instead of engine buffers: bytes [0, 256) hold the kernel's
+// arrival counter, the rest five partial sums per block, one block per
+// kThreads entries of the longer vector.
+namespace {
+constexpr int64_t kStaticMonitorBlocks = NK_MONITOR_STATIC_MAX / nk::kThreads;
+constexpr size_t kStaticMonitorBytes = 256 + size_t(kStaticMonitorBlocks) * 5 * sizeof(double);
+static __device__ __align__(256) unsigned char g_monitor_scratch[kStaticMonitorBytes];
+
+// Device address of g_monitor_scratch on the current device.  In host code the
+// symbol is only a stand-in; its device address is looked up once per device.
+unsigned char *static_monitor_scratch() {
+    constexpr int kMaxDevices = 64;
+    static std::mutex lock;
+    static unsigned char *address[kMaxDevices] = {};
+    int dev = 0;
+    nk::cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= kMaxDevices)
+        throw nk::Error(NK_ERR_UNSUPPORTED, "device index beyond the static scratch table");
+    std::lock_guard<std::mutex> hold(lock);
+    if (!address[dev]) {
+        void *p = nullptr;
+        nk::cuda_check(cudaGetSymbolAddress(&p, g_monitor_scratch), "cudaGetSymbolAddress");
+        address[dev] = static_cast<unsigned char *>(p);
+    }
+    return address[dev];
+}
+} // namespace
+
+nk_status nk_monitor_static(int64_t n, int64_t m, const double *x, const double *y,
+                            const double *ax, const double *aty, const double *qx,
+                            const double *c, const double *q, const double *lb, const double *ub,
+                            const double *rl, const double *ru, double cscale, double *result,
+                            void *stream) {
+    return guard([&] {
+        if (n < 0 || m < 0)
+            throw nk::Error(NK_ERR_INVALID, "negative vector length");
+        if (n > NK_MONITOR_STATIC_MAX || m > NK_MONITOR_STATIC_MAX)
+            throw nk::Error(NK_ERR_INVALID,
+                            "nk_monitor_static: n and m must be at most NK_MONITOR_STATIC_MAX "
+                            "(4194304 entries); its fixed scratch holds no more block partials");
+        if (!result || (n && (!x || !aty || !c || !q || !lb || !ub)) ||
+            (m && (!y || !ax || !rl || !ru)))
+            throw nk::Error(NK_ERR_INVALID, "null vector");
+        auto s = static_cast<cudaStream_t>(stream);
+        unsigned char *base = static_monitor_scratch();
+        auto *arrive = reinterpret_cast<unsigned *>(base);
+        auto *partial = reinterpret_cast<double *>(base + 256);
+        const int64_t top = std::max(n, m);
+        if (top == 0) {
+            nk::cuda_check(cudaMemsetAsync(result, 0, sizeof(double), s), "result");
+            return;
+        }
+        const int blocks = int((top + nk::kThreads - 1) / nk::kThreads);
+        // a call that ended early must not leave a stale count behind
+        nk::cuda_check(cudaMemsetAsync(arrive, 0, sizeof(unsigned), s), "clear counter");
+        nk::monitor_kernel<<<blocks, nk::kThreads, 0, s>>>(n, m, x, y, ax, aty, qx, c, q, lb, ub,
+                                                           rl, ru, cscale, partial, arrive, result);
+        nk::cuda_check(cudaGetLastError(), "monitor launch");
+    });
+}
+
 nk_status nk_pdhg_candidates(nk_pdhg *h, double *x, double *y, double *xa, double *ya) {
     return guard([&] {
         NK_HANDLE

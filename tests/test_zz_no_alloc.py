@@ -1,0 +1,76 @@
+"""nk_monitor_static: the KKT proxy for callers that may not allocate device memory.
+
+Some callers of this library cannot call cudaMalloc: a host application that
+gives all device memory to its own pool or admission budget, or a
+latency-critical loop where an allocation would synchronise the device.  For
+them nk_monitor_static runs the monitor kernel on a fixed array inside the
+library.  This test feeds it the engine's own iterates (device vectors the test
+allocates with torch) and checks it against nk_pdhg_monitor, the existing
+entry point, on two calls in a row, plus its size limit.
+
+The file name sorts last so that a run stopping at the first failure has run
+every other test first; it also passes alone in a fresh process.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from niryukti_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+MAX = 4194304  # NK_MONITOR_STATIC_MAX
+
+
+def bind(lib):
+    D = C.POINTER(C.c_double)
+    f = lib.nk_monitor_static
+    f.argtypes = [C.c_int64, C.c_int64] + [C.c_void_p] * 11 + [C.c_double, C.c_void_p,
+                                                                C.c_void_p]
+    f.restype = C.c_int
+    return f
+
+
+def test_static_monitor_matches_engine_monitor(gpu):
+    import torch
+    model = synth.random_lp(m=3000, n=7000, per_col=5, seed=13)
+    model.q = np.where(np.arange(model.n) % 7 == 0, 0.5, 0.0)  # diagonal QP terms too
+    engine = gpu
+    lib = engine.library()
+    f = bind(lib)
+    b = engine.PdhgBackend(model, adaptive=True)
+    b.advance(300, 0.05, 0.05)
+    expected = b.monitor()  # min over the current and averaged points
+    x, y, xa, ya = b.candidates()
+    dev = torch.device("cuda", 0)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)
+    at_ptr, at_idx, at_val = synth.transpose(model.ptr, model.idx, model.val, model.m, model.n)
+    cscale = max(1.0, float(np.max(1 + np.abs(model.c))))
+    const = {k: t(getattr(model, k)) for k in ("c", "q", "lb", "ub", "rl", "ru")}
+    stream = torch.cuda.current_stream(dev)
+    outs = []
+    for px, py in ((x, y), (xa, ya), (x, y)):
+        ax = synth.csr_matvec(model.ptr, model.idx, model.val, px, model.m)
+        aty = synth.csr_matvec(at_ptr, at_idx, at_val, py, model.n)
+        dx, dy, dax, daty = t(px), t(py), t(ax), t(aty)
+        res = torch.full((1,), np.nan, dtype=torch.float64, device=dev)
+        status = f(model.n, model.m, dx.data_ptr(), dy.data_ptr(), dax.data_ptr(),
+                   daty.data_ptr(), None, const["c"].data_ptr(), const["q"].data_ptr(),
+                   const["lb"].data_ptr(), const["ub"].data_ptr(), const["rl"].data_ptr(),
+                   const["ru"].data_ptr(), cscale, res.data_ptr(), C.c_void_p(stream.cuda_stream))
+        assert status == 0, lib.nk_last_error().decode()
+        stream.synchronize()
+        outs.append(float(res.item()))
+    assert all(np.isfinite(outs))
+    assert outs[2] == outs[0]  # the shared scratch carries nothing from call to call
+    got = min(outs[:2])
+    assert abs(got - expected) <= 1e-10 * (1 + abs(expected)), (got, expected, outs)
+
+
+def test_static_monitor_rejects_oversized_input(gpu):
+    lib = gpu.library()
+    f = bind(lib)
+    status = f(MAX + 1, 10, *([None] * 11), 1.0, None, None)
+    assert status == 1  # NK_ERR_INVALID
+    assert "NK_MONITOR_STATIC_MAX" in lib.nk_last_error().decode()
