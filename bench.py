@@ -135,10 +135,20 @@ def dist_setup():
 
 
 def build_model(args):
+    """Config 2 (m=1e6, n=2e6, nnz=2e7), or the same generator scaled by
+    --scale (profiling captures use a smaller, still larger-than-L2 case)."""
     from niryukti_b200 import synth
-    if args.small:
-        return synth.power_law_lp(m=100_000, n=200_000, nnz=2_000_000, seed=2)
-    return synth.power_law_lp(seed=2)
+    f = 0.1 if args.small else args.scale
+    if f == 1.0:
+        return synth.power_law_lp(seed=2)
+    return synth.power_law_lp(m=int(1_000_000 * f), n=int(2_000_000 * f),
+                              nnz=int(20_000_000 * f), seed=2)
+
+
+def workload_name(args):
+    f = 0.1 if args.small else args.scale
+    return ("config2_power_law_lp_m1e6_n2e6_nnz2e7" if f == 1.0 else
+            f"config2_shape_scaled_{f:g}")
 
 
 # ---------------------------------------------------------------- CPU arm
@@ -174,7 +184,8 @@ def cpu_child(args):
 def run_cpu_child(args):
     cmd = [sys.executable, str(pathlib.Path(__file__).resolve()), "--cpu-child",
            "--cpu-seconds", str(args.cpu_seconds), "--cpu-threads", str(args.cpu_threads),
-           "--cpu-trials", str(args.cpu_trials)] + (["--small"] if args.small else [])
+           "--cpu-trials", str(args.cpu_trials), "--scale", str(args.scale)] + \
+        (["--small"] if args.small else [])
     env = dict(os.environ, OMP_NUM_THREADS=str(args.cpu_threads))
     out = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=1800)
     if out.returncode != 0:
@@ -211,7 +222,7 @@ def reference_arm(args, world, rank):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "config2_power_law_lp_m1e6_n2e6_nnz2e7", "m": m, "n": n,
+            "config": {"workload": workload_name(args), "m": m, "n": n,
                        "nnz": nnz, "trials_per_step": per, "seed": 2},
             "iterations_per_s": rate,
             "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": kind,
@@ -227,8 +238,7 @@ def solve_models(args):
     from niryukti_b200 import synth
     c1 = synth.random_lp(m=2000, n=5000, per_col=5, seed=1)
     c2 = build_model(args)
-    return {"config1_lp_m2000_n5000": c1, "config2_power_law_lp" + ("_small" if args.small else
-                                                                     "_m1e6_n2e6_nnz2e7"): c2}
+    return {"config1_lp_m2000_n5000": c1, workload_name(args): c2}
 
 
 def reference_solve(model, budget, threads):
@@ -291,7 +301,8 @@ def solve_section(args):
     if not args.no_cpu:
         cmd = [sys.executable, str(pathlib.Path(__file__).resolve()), "--solve-child",
                "--cpu-threads", str(args.cpu_threads), "--cpu-solve-seconds",
-               str(args.cpu_solve_seconds)] + (["--small"] if args.small else [])
+               str(args.cpu_solve_seconds), "--scale", str(args.scale)] + \
+            (["--small"] if args.small else [])
         env = dict(os.environ, OMP_NUM_THREADS=str(args.cpu_threads))
         try:
             out = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=1800)
@@ -302,6 +313,89 @@ def solve_section(args):
             for name in res:
                 res[name]["reference_cpu"] = {"error": str(exc)[-300:]}
     return res
+
+
+# ---------------------------------------------------------------- batch (config 4)
+def batch_models(args):
+    from niryukti_b200 import synth
+    return synth.batch_instances(count=args.batch_count, m_lo=500, m_hi=args.batch_m_hi,
+                                 qp_frac=0.2, seed=4)
+
+
+def batch_section(args):
+    """Config 4: 512 uneven LP/QP instances (m log-uniform in [500, 50000],
+    n = 2m, 20% QPs) solved to 1e-6 relative KKT by the batched engine (FP32
+    matrices, FP64 iterates and reductions), beside the plain FP64 solve run
+    instance by instance on the same GPU (a stratified sample, timed one by
+    one) and the reference's CPU solve of the same sample."""
+    from concurrent.futures import ThreadPoolExecutor
+    from niryukti_b200 import batch as nb, solver
+    t0 = time.perf_counter()
+    models = batch_models(args)
+    gen_s = time.perf_counter() - t0
+    opts = dict(tol=1e-6, matrix_precision=args.batch_precision, iteration_limit=400000,
+                time_limit=600)
+    with nb.BatchEngine(**opts) as eng:
+        w0 = time.perf_counter()
+        with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as pool:
+            items = list(pool.map(eng.prepare, models))
+        prep_s = time.perf_counter() - w0
+        g0 = time.perf_counter()
+        for k, it in enumerate(items):
+            if not eng.admit(it, k):
+                raise MemoryError("config-4 batch does not fit the device budget")
+        info = eng.info()
+        results = {}
+        while len(results) < len(models):
+            for k in eng.step(checks=1000000):
+                results[k] = eng.result(k)
+        gpu_s = time.perf_counter() - g0
+    statuses = {}
+    for r in results.values():
+        statuses[r["status"]] = statuses.get(r["status"], 0) + 1
+    iters = sorted(r["iterations"] for r in results.values())
+    worst = max(r["kkt"] for r in results.values())
+    # the plain FP64 single-instance solve on a stratified sample (by size)
+    order = sorted(range(len(models)), key=lambda k: models[k].nnz)
+    sample = [order[int(q * (len(order) - 1))] for q in np.linspace(0, 1, args.batch_sample)]
+    plain = []
+    for k in sample:
+        p0 = time.perf_counter()
+        r = solver.solve(models[k], tol=1e-6, iteration_limit=400000, time_limit=600)
+        plain.append({"instance": k, "m": models[k].m, "nnz": models[k].nnz,
+                      "seconds": time.perf_counter() - p0, "status": r["status"],
+                      "iterations": r["iterations"],
+                      "objective_diff": abs(r["objective"] - results[k]["objective"]) /
+                      (1 + abs(r["objective"]))})
+    # the sample's share of the batch work: scale its time to all instances by nnz
+    sample_nnz = sum(models[k].nnz for k in sample)
+    total_nnz = sum(m.nnz for m in models)
+    plain_s = sum(p["seconds"] for p in plain) * total_nnz / sample_nnz
+    out = {"workload": f"config4_{len(models)}_uneven_lp_qp_m500_{args.batch_m_hi}",
+           "instances": len(models), "qp": sum(1 for m in models if m.is_qp()),
+           "total_nnz": total_nnz, "precision": args.batch_precision, "tol": 1e-6,
+           "statuses": statuses, "worst_certified_kkt": worst,
+           "iterations": {"min": iters[0], "median": iters[len(iters) // 2], "max": iters[-1]},
+           "generate_s": gen_s, "prepare_s_parallel": prep_s, "gpu_phase_s": gpu_s,
+           "solves_per_s": len(models) / gpu_s,
+           "solves_per_s_with_prepare": len(models) / (gpu_s + prep_s),
+           "kernel_variants": {"primal": info["primal_variant"], "dual": info["dual_variant"]},
+           "plain_fp64_one_by_one": {"sample": plain, "extrapolated_s": plain_s,
+                                     "solves_per_s": len(models) / plain_s},
+           "speedup_vs_plain": plain_s / gpu_s}
+    if not args.no_cpu:
+        from oracle import oracle as orc
+        if orc.REF_SO.exists():
+            cpu = []
+            for k in sample[: max(1, len(sample) // 2)]:
+                r = reference_solve(models[k], 120.0, args.cpu_threads)
+                cpu.append({"instance": k, "seconds": r["seconds"], "status": r["status"]})
+            cnnz = sum(models[c["instance"]].nnz for c in cpu)
+            cpu_s = sum(c["seconds"] for c in cpu) * total_nnz / cnnz
+            out["reference_cpu_one_by_one"] = {"sample": cpu, "extrapolated_s": cpu_s,
+                                               "solves_per_s": len(models) / cpu_s,
+                                               "threads": args.cpu_threads}
+    return out
 
 
 # ---------------------------------------------------------------- engine arm
@@ -416,8 +510,7 @@ def engine_arm(args, world, rank, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32-matrix/f64-iterates",
             "data": "synthetic (seeded power-law LP, numpy PCG64 seed 2)",
-            "config": {"workload": "config2_power_law_lp_m1e6_n2e6_nnz2e7" if not args.small
-                       else "config2_small", "m": m, "n": n, "nnz": nnz,
+            "config": {"workload": workload_name(args), "m": m, "n": n, "nnz": nnz,
                        "trials_per_step": TRIALS_PER_STEP, "precision": args.precision,
                        "adaptive": True, "graphs": True, "parallelism": f"replicas{world}",
                        "l2": "inputs larger than L2 (about 730 MB per iteration)"},
@@ -433,6 +526,8 @@ def engine_arm(args, world, rank, local):
     del g
     if not args.no_solve:
         line["solve"] = solve_section(args)
+    if not args.no_batch:
+        line["batch"] = batch_section(args)
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
@@ -446,6 +541,8 @@ def main():
     ap.add_argument("--impl", default="nk", choices=["nk", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "fp32"])
     ap.add_argument("--small", action="store_true", help="10x smaller instance (testing)")
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="scale m, n and nnz of the config-2 generator (profiling cases)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-child", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -460,6 +557,13 @@ def main():
     ap.add_argument("--cpu-solve-seconds", type=float, default=30.0,
                     help="time budget of the reference's config-2 CPU solve")
     ap.add_argument("--solve-child", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--no-batch", action="store_true", help="skip the config-4 batched solves")
+    ap.add_argument("--batch-only", action="store_true",
+                    help="print only the config-4 batched-solve section")
+    ap.add_argument("--batch-count", type=int, default=512)
+    ap.add_argument("--batch-m-hi", type=int, default=50000)
+    ap.add_argument("--batch-sample", type=int, default=6)
+    ap.add_argument("--batch-precision", default="mixed", choices=["fp64", "mixed", "fp32"])
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per launch of the top kernel from an ncu capture")
     args = ap.parse_args()
@@ -469,6 +573,9 @@ def main():
         return cpu_child(args)
     if args.solve_child:
         return solve_child(args)
+    if args.batch_only:
+        print(json.dumps({"batch": batch_section(args)}))
+        return
     world, rank, local = dist_setup()
     if args.impl == "reference":
         return reference_arm(args, world, rank)

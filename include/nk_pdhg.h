@@ -230,6 +230,66 @@ nk_status nk_solve(const nk_model *model, const nk_solve_options *options,
 
 /* cuda_available / cuda_description / hardware_info --
  * include/vantage/vantage.hpp:76,145-146, src/cuda.cu:1267-1287. */
+/* ------------------------------------------------------------------ batch
+ * Many independent LP / convex-QP solves advanced together on one GPU, each
+ * with its own step sizes, adaptive acceptance, restarts, primal weight and
+ * termination (the driver of nk_solve per instance).  The reference has one
+ * batching entry, cuda_batch_relaxations (src/cuda.cu:1136-1266: box variants
+ * of a single LP, fixed steps, no restarts, no QP); this family replaces it
+ * for uneven, unrelated instances and is what the serving loop runs on.
+ *
+ * Instances keep their own device storage and join a work list of
+ * (instance, 32-row chunk) pairs; one trial of the batch is three kernel
+ * launches for all instances, captured in a CUDA graph per check interval.
+ * Kernel variants (unroll depth, CTA size) are chosen by an autotuner that
+ * times them on the batch itself.  Instances join and leave at check
+ * boundaries.  Handles are single-threaded; nk_batch_prepare is thread-safe
+ * and touches no device, so requests can be prepared while the batch runs. */
+typedef struct {
+    double tol, time_limit;   /* per instance (1e-6, 60 s from admission) */
+    int64_t iteration_limit;  /* per instance (100000) */
+    int check_every;          /* trials between candidate checks (100) */
+    int presolve, scaling_combined, scaling_passes, adaptive, restart, graphs;
+    int autotune;             /* time kernel variants on the live batch (1) */
+    int precision;            /* NK_PRECISION_FP64, or MIXED (the default): FP32 values
+                                 until an instance's KKT reaches phase_tol or stalls,
+                                 then an FP64 refinement restarted from its best point */
+    double phase_tol;         /* MIXED phase target (0: 10 * tol) */
+    double memory_budget;     /* admission budget in bytes (0: 80% of free memory) */
+    int capacity;             /* instance slots (4096) */
+} nk_batch_options;
+typedef struct nk_batch nk_batch;
+typedef struct nk_batch_item nk_batch_item;
+
+void nk_batch_defaults(nk_batch_options *options);
+nk_status nk_batch_create(const nk_batch_options *options, nk_batch **out);
+void nk_batch_destroy(nk_batch *batch);
+/* The reference's device-memory estimate of a model (src/solver.cpp:227-228). */
+nk_status nk_batch_estimate(const nk_model *model, double *bytes);
+/* Presolve, scale, check the start point and lay out one instance (host only).
+ * *device_bytes: what admitting it will take (0 if it terminated already). */
+nk_status nk_batch_prepare(const nk_model *model, const nk_batch_options *options,
+                           nk_batch_item **out, double *device_bytes);
+void nk_batch_item_free(nk_batch_item *item);
+/* Admits a prepared instance under `id`: *admitted = 1 (the batch owns the
+ * item now) or 0 (over the memory budget or no free slot; the caller keeps it). */
+nk_status nk_batch_admit(nk_batch *batch, nk_batch_item *item, int64_t id, int *admitted);
+/* Runs up to `checks` check intervals, stopping early once some instance
+ * finished; their ids go to finished[0 .. *count). */
+nk_status nk_batch_step(nk_batch *batch, int checks, int64_t *finished, int capacity, int *count);
+/* Result of a finished instance (x: its n, y: its m original entries; either
+ * may be NULL); releases its slot and device memory. */
+nk_status nk_batch_result(nk_batch *batch, int64_t id, nk_solve_result *result, double *x,
+                          double *y);
+nk_status nk_batch_info(nk_batch *batch, int *active, double *used_bytes, double *budget_bytes,
+                        int *variant_primal, int *variant_dual);
+/* Profiling (no reference counterpart): mean time of `trials` batch trials,
+ * and the algorithmic bytes of one trial's two SpMV passes over all instances. */
+nk_status nk_batch_time_trials(nk_batch *batch, int trials, double *ms, int64_t *bytes_per_trial);
+/* Profiling (no reference counterpart): the autotuner's best single-launch
+ * times of the batched primal and dual kernels (0 before tuning). */
+nk_status nk_batch_kernel_times(nk_batch *batch, double *primal_ms, double *dual_ms);
+
 /* KKT proxy without any device allocation.  No counterpart in the reference:
  * it exists for callers that must not allocate device memory themselves --
  * a host application that hands all device memory to its own pool or budget

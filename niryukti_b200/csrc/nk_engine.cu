@@ -19,9 +19,11 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <numeric>
+#include <set>
 #include <vector>
 
 #ifndef NK_SPLIT
@@ -1205,6 +1207,7 @@ Engine *create_engine(const nk_csr *Ah, const nk_csr *Qh, const double *hc, cons
 } // namespace nk
 
 #include "nk_solve.cuh"
+#include "nk_batch.cuh"
 
 namespace nk {
 // Copies a caller model (C ABI) into the host representation, after the
@@ -1675,6 +1678,194 @@ nk_status nk_solve(const nk_model *model, const nk_solve_options *o, nk_solve_re
             std::memcpy(x, R.x.data(), size_t(n) * 8);
         if (y && R.y.size() == size_t(m))
             std::memcpy(y, R.y.data(), size_t(m) * 8);
+    });
+}
+
+// ------------------------------------------------------------------ batch
+struct nk_batch {
+    nk::Batch b;
+    explicit nk_batch(const nk::BatchOptions &o) : b(o) {}
+};
+struct nk_batch_item {
+    std::unique_ptr<nk::BatchItem> item;
+};
+
+void nk_batch_defaults(nk_batch_options *o) {
+    if (!o)
+        return;
+    *o = nk_batch_options{};
+    o->tol = 1e-6;
+    o->time_limit = 60;
+    o->iteration_limit = 100000;
+    o->check_every = 100;
+    o->presolve = 1;
+    o->scaling_passes = 5;
+    o->adaptive = 1;
+    o->restart = 1;
+    o->graphs = 1;
+    o->autotune = 1;
+    o->precision = NK_PRECISION_MIXED;
+    o->capacity = 4096;
+}
+
+static nk::BatchOptions batch_options(const nk_batch_options *o) {
+    if (!o)
+        throw nk::Error(NK_ERR_INVALID, "null batch options");
+    if (!(o->tol > 0) || o->check_every <= 0 || o->iteration_limit < 0 || !(o->time_limit >= 0) ||
+        o->scaling_passes < 0 || o->precision < 0 || o->precision > 2 || o->memory_budget < 0)
+        throw nk::Error(NK_ERR_INVALID, "invalid batch options");
+    nk::BatchOptions b;
+    b.tol = o->tol;
+    b.time_limit = o->time_limit;
+    b.iteration_limit = o->iteration_limit;
+    b.check_every = o->check_every;
+    b.prepare.presolve = o->presolve != 0;
+    b.prepare.scaling = o->scaling_combined ? "combined" : "ruiz";
+    b.prepare.scaling_passes = o->scaling_passes;
+    b.adaptive = o->adaptive != 0;
+    b.restart = o->restart != 0;
+    b.graphs = o->graphs != 0;
+    b.autotune = o->autotune != 0;
+    b.precision = o->precision;
+    b.phase_tol = o->phase_tol;
+    b.memory_budget = o->memory_budget;
+    b.capacity = o->capacity;
+    return b;
+}
+
+nk_status nk_batch_create(const nk_batch_options *o, nk_batch **out) {
+    return guard([&] {
+        if (!out)
+            throw nk::Error(NK_ERR_INVALID, "null output handle");
+        *out = nullptr;
+        *out = new nk_batch(batch_options(o));
+    });
+}
+void nk_batch_destroy(nk_batch *h) { delete h; }
+
+nk_status nk_batch_estimate(const nk_model *model, double *bytes) {
+    return guard([&] {
+        if (!bytes)
+            throw nk::Error(NK_ERR_INVALID, "null output");
+        *bytes = nk::batch_estimate(nk::host_model(model));
+    });
+}
+
+nk_status nk_batch_prepare(const nk_model *model, const nk_batch_options *o, nk_batch_item **out,
+                           double *device_bytes) {
+    return guard([&] {
+        if (!out)
+            throw nk::Error(NK_ERR_INVALID, "null output handle");
+        *out = nullptr;
+        auto opts = batch_options(o);
+        auto item = std::make_unique<nk_batch_item>();
+        item->item = nk::batch_prepare(nk::host_model(model), opts);
+        if (device_bytes)
+            *device_bytes = item->item->decided ? 0. : double(item->item->bytes);
+        *out = item.release();
+    });
+}
+void nk_batch_item_free(nk_batch_item *item) { delete item; }
+
+nk_status nk_batch_admit(nk_batch *h, nk_batch_item *item, int64_t id, int *admitted) {
+    return guard([&] {
+        if (!h || !item || !item->item || !admitted)
+            throw nk::Error(NK_ERR_INVALID, "null argument");
+        *admitted = h->b.admit(item->item, id) ? 1 : 0;
+        if (*admitted)
+            delete item;
+    });
+}
+
+nk_status nk_batch_step(nk_batch *h, int checks, int64_t *finished, int capacity, int *count) {
+    return guard([&] {
+        if (!h || !count || checks < 0 || capacity < 0 || (capacity && !finished))
+            throw nk::Error(NK_ERR_INVALID, "invalid argument");
+        auto done = h->b.step(checks);
+        if (int(done.size()) > capacity)
+            throw nk::Error(NK_ERR_INVALID, "finished-id buffer too small");
+        for (size_t k = 0; k < done.size(); ++k)
+            finished[k] = done[k];
+        *count = int(done.size());
+    });
+}
+
+nk_status nk_batch_result(nk_batch *h, int64_t id, nk_solve_result *result, double *x, double *y) {
+    return guard([&] {
+        if (!h || !result)
+            throw nk::Error(NK_ERR_INVALID, "null argument");
+        nk::SolveReport R = h->b.take(id);
+        nk_solve_result &r = *result;
+        r = nk_solve_result{};
+        r.status = R.status;
+        r.iterations = R.iterations;
+        r.restarts = R.restarts;
+        r.rejected_steps = R.rejected;
+        r.weight_updates = R.weight_updates;
+        r.device_checks = R.device_checks;
+        r.host_checks = R.host_checks;
+        r.removed_rows = R.removed_rows;
+        r.removed_columns = R.removed_columns;
+        r.preprocess_seconds = R.preprocess;
+        r.transfer_seconds = R.transfer;
+        r.iteration_seconds = R.iteration;
+        r.verification_seconds = R.verification;
+        r.seconds = R.preprocess + R.transfer + R.iteration + R.verification;
+        r.objective = R.accuracy.objective;
+        r.kkt = R.accuracy.kkt;
+        r.primal = R.accuracy.primal;
+        r.dual = R.accuracy.dual;
+        r.gap = R.accuracy.gap;
+        r.lower_bound = R.accuracy.lower_bound;
+        r.phase_iterations = R.mixed_iterations;
+        r.refine_iterations = R.refine_iterations;
+        r.phase_objective = R.mixed.objective;
+        r.phase_kkt = R.mixed.kkt;
+        r.phase_primal = R.mixed.primal;
+        r.phase_dual = R.mixed.dual;
+        r.phase_gap = R.mixed.gap;
+        for (int k = 0; k < 9; ++k)
+            r.reached[k] = R.reached[k];
+        if (x && !R.x.empty())
+            std::memcpy(x, R.x.data(), R.x.size() * 8);
+        if (y && !R.y.empty())
+            std::memcpy(y, R.y.data(), R.y.size() * 8);
+    });
+}
+
+nk_status nk_batch_info(nk_batch *h, int *active, double *used_bytes, double *budget_bytes,
+                        int *variant_primal, int *variant_dual) {
+    return guard([&] {
+        if (!h)
+            throw nk::Error(NK_ERR_INVALID, "null handle");
+        if (active)
+            *active = h->b.active();
+        if (used_bytes)
+            *used_bytes = h->b.used();
+        if (budget_bytes)
+            *budget_bytes = h->b.budget();
+        if (variant_primal)
+            *variant_primal = h->b.variant_primal();
+        if (variant_dual)
+            *variant_dual = h->b.variant_dual();
+    });
+}
+
+nk_status nk_batch_kernel_times(nk_batch *h, double *primal_ms, double *dual_ms) {
+    return guard([&] {
+        if (!h || !primal_ms || !dual_ms)
+            throw nk::Error(NK_ERR_INVALID, "null argument");
+        *primal_ms = h->b.tuned_ms_primal();
+        *dual_ms = h->b.tuned_ms_dual();
+    });
+}
+nk_status nk_batch_time_trials(nk_batch *h, int trials, double *ms, int64_t *bytes_per_trial) {
+    return guard([&] {
+        if (!h || !ms || trials < 0)
+            throw nk::Error(NK_ERR_INVALID, "invalid argument");
+        *ms = h->b.time_trials(trials);
+        if (bytes_per_trial)
+            *bytes_per_trial = h->b.matrix_bytes_per_trial();
     });
 }
 }

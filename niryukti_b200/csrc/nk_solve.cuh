@@ -815,11 +815,10 @@ inline SolveReport solve(const HostModel &original, const SolveSettings &S) {
     Driver drv(*D, verifier, o, R, start, R.accuracy.kkt);
     drv.step = step;
     drv.weight = weight;
-    bool finished = false;
     Accuracy best;
     if (phased) {
         double target = S.phase_tol > 0 ? S.phase_tol : 10 * o.tol;
-        finished = drv.run(S.refine ? target : o.tol, !S.refine, o.iteration_limit);
+        drv.run(S.refine ? target : o.tol, !S.refine, o.iteration_limit);
         best = drv.best;
         R.mixed_iterations = R.iterations;
         R.mixed_seconds = since(start);
@@ -848,12 +847,12 @@ inline SolveReport solve(const HostModel &original, const SolveSettings &S) {
             fine.best = best;
             R.status = NK_SOLVE_ITERATION_LIMIT;
             int64_t before = R.iterations;
-            finished = fine.run(o.tol, true, o.iteration_limit);
+            fine.run(o.tol, true, o.iteration_limit);
             R.refine_iterations = R.iterations - before;
             best = fine.best;
         }
     } else {
-        finished = drv.run(o.tol, true, o.iteration_limit);
+        drv.run(o.tol, true, o.iteration_limit);
         best = drv.best;
     }
     if (R.status != NK_SOLVE_OPTIMAL && R.status != NK_SOLVE_INFEASIBLE) {
@@ -871,7 +870,6 @@ inline SolveReport solve(const HostModel &original, const SolveSettings &S) {
         }
         R.verification += since(tick);
     }
-    (void)finished;
     R.seconds = since(start);
     return R;
 }
