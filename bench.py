@@ -241,7 +241,7 @@ def solve_models(args):
     return {"config1_lp_m2000_n5000": c1, workload_name(args): c2}
 
 
-def reference_solve(model, budget, threads):
+def reference_solve(model, budget, threads, iteration_limit=10**9):
     """The reference's own solve (vantage::solve, method pdhg, device cpu) from
     oracle/_ref, with its per-check verbose lines turned into times to each KKT
     decade; None when the reference build is absent."""
@@ -256,7 +256,7 @@ def reference_solve(model, budget, threads):
         os.dup2(fd, 2)  # the reference prints its check lines on stderr
         r = orc.Reference().model(model).solve(method="pdhg", device="cpu", verbose=True,
                                                time_limit=budget, threads=threads,
-                                               iteration_limit=10**9)
+                                               iteration_limit=iteration_limit)
     finally:
         os.dup2(saved, 2)
         os.close(saved)
@@ -333,7 +333,9 @@ def batch_section(args):
     t0 = time.perf_counter()
     models = batch_models(args)
     gen_s = time.perf_counter() - t0
-    opts = dict(tol=1e-6, matrix_precision=args.batch_precision, iteration_limit=400000,
+    # the reference's default limits (100000 iterations; the time limit raised
+    # from 60 s so that it never binds here), the same for both forms
+    opts = dict(tol=1e-6, matrix_precision=args.batch_precision, iteration_limit=100000,
                 time_limit=600)
     with nb.BatchEngine(**opts) as eng:
         w0 = time.perf_counter()
@@ -345,10 +347,11 @@ def batch_section(args):
             if not eng.admit(it, k):
                 raise MemoryError("config-4 batch does not fit the device budget")
         info = eng.info()
-        results = {}
+        results, finish_t = {}, {}
         while len(results) < len(models):
             for k in eng.step(checks=1000000):
                 results[k] = eng.result(k)
+                finish_t[k] = time.perf_counter() - g0
         gpu_s = time.perf_counter() - g0
     statuses = {}
     for r in results.values():
@@ -361,16 +364,16 @@ def batch_section(args):
     plain = []
     for k in sample:
         p0 = time.perf_counter()
-        r = solver.solve(models[k], tol=1e-6, iteration_limit=400000, time_limit=600)
+        r = solver.solve(models[k], tol=1e-6, iteration_limit=100000, time_limit=600)
         plain.append({"instance": k, "m": models[k].m, "nnz": models[k].nnz,
                       "seconds": time.perf_counter() - p0, "status": r["status"],
                       "iterations": r["iterations"],
                       "objective_diff": abs(r["objective"] - results[k]["objective"]) /
                       (1 + abs(r["objective"]))})
-    # the sample's share of the batch work: scale its time to all instances by nnz
-    sample_nnz = sum(models[k].nnz for k in sample)
+    # the sample sits at evenly spaced size quantiles, so its mean time per
+    # instance times the instance count estimates the one-by-one total
     total_nnz = sum(m.nnz for m in models)
-    plain_s = sum(p["seconds"] for p in plain) * total_nnz / sample_nnz
+    plain_s = sum(p["seconds"] for p in plain) / len(plain) * len(models)
     out = {"workload": f"config4_{len(models)}_uneven_lp_qp_m500_{args.batch_m_hi}",
            "instances": len(models), "qp": sum(1 for m in models if m.is_qp()),
            "total_nnz": total_nnz, "precision": args.batch_precision, "tol": 1e-6,
@@ -382,20 +385,114 @@ def batch_section(args):
            "kernel_variants": {"primal": info["primal_variant"], "dual": info["dual_variant"]},
            "plain_fp64_one_by_one": {"sample": plain, "extrapolated_s": plain_s,
                                      "solves_per_s": len(models) / plain_s},
-           "speedup_vs_plain": plain_s / gpu_s}
+           "speedup_vs_plain": plain_s / gpu_s,
+           # per instance: m, QP?, status, iterations, reduced-precision iterations,
+           # seconds from admission to its result
+           "per_instance": [[models[k].m, int(models[k].is_qp()), results[k]["status"][:3],
+                             results[k]["iterations"], results[k]["phase_iterations"],
+                             round(finish_t[k], 2)] for k in range(len(models))],
+           "finished_by_time": {f"{q}%": sorted(finish_t.values())[
+               min(len(finish_t) - 1, int(q / 100 * len(finish_t)))] for q in (50, 90, 99, 100)}}
     if not args.no_cpu:
         from oracle import oracle as orc
         if orc.REF_SO.exists():
             cpu = []
-            for k in sample[: max(1, len(sample) // 2)]:
-                r = reference_solve(models[k], 120.0, args.cpu_threads)
-                cpu.append({"instance": k, "seconds": r["seconds"], "status": r["status"]})
-            cnnz = sum(models[c["instance"]].nnz for c in cpu)
-            cpu_s = sum(c["seconds"] for c in cpu) * total_nnz / cnnz
+            for k in sample[: args.batch_cpu_sample]:
+                r = reference_solve(models[k], args.cpu_solve_seconds, args.cpu_threads, 100000)
+                cpu.append({"instance": k, "m": models[k].m, "seconds": r["seconds"],
+                            "status": r["status"], "iterations": r["iterations"]})
+            cpu_s = sum(c["seconds"] for c in cpu) / len(cpu) * len(models)
             out["reference_cpu_one_by_one"] = {"sample": cpu, "extrapolated_s": cpu_s,
                                                "solves_per_s": len(models) / cpu_s,
                                                "threads": args.cpu_threads}
     return out
+
+
+# ---------------------------------------------------------------- serving (config 5)
+def serve_section(args):
+    """Config 5: Poisson arrivals at --serve-rate requests/s for --serve-seconds,
+    each request drawn from a pool of config-4-style instances with m
+    log-uniform in [500, 200000]; served by continuous batching (admission by
+    device-memory footprint under a 150 GB budget), and by the plain FP64
+    solve one request at a time on the same arrival stream.  Reported over the
+    arrival window plus a drain of --serve-drain seconds: completed solves per
+    second and the latency percentiles of the completed requests; requests
+    still open at the end are counted, not timed."""
+    from niryukti_b200 import serve, solver
+    pool = synth_pool(args)
+    rng = np.random.default_rng(6)
+    t, arrivals = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / args.serve_rate)
+        if t >= args.serve_seconds:
+            break
+        arrivals.append(t)
+    picks = rng.integers(0, len(pool), len(arrivals))
+    horizon = args.serve_seconds + args.serve_drain
+
+    def summary(lat, done, t_total):
+        lat = sorted(lat)
+        pct = (lambda q: lat[min(len(lat) - 1, int(q * len(lat)))] if lat else None)
+        return {"offered": len(arrivals), "completed": done, "open_at_end": len(arrivals) - done,
+                "solves_per_s": done / t_total, "p50_s": pct(.5), "p95_s": pct(.95),
+                "p99_s": pct(.99)}
+
+    # served: a feeder submits at the arrival times
+    svc = serve.SolveService(memory_budget=150e9, matrix_precision="mixed",
+                             prepare_workers=os.cpu_count() or 8,
+                             iteration_limit=100000, time_limit=horizon)
+    lat, statuses = [], {}
+    futs = []
+    t0 = time.perf_counter()
+    for a, k in zip(arrivals, picks):
+        delay = t0 + a - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        f = svc.submit(pool[int(k)])
+        f.arrival = a
+        futs.append(f)
+    deadline = t0 + horizon
+    for f in futs:
+        left = deadline - time.perf_counter()
+        if left <= 0:
+            break
+        try:
+            r = f.result(timeout=left)
+        except Exception:
+            continue
+        statuses[r["status"]] = statuses.get(r["status"], 0) + 1
+        lat.append(r["latency_s"])
+    done_served = len(lat)
+    served = summary(lat, done_served, horizon)
+    served["statuses"] = statuses
+    served["engine"] = {k: v for k, v in svc.stats().items() if k != "budget_bytes"}
+    svc.close()
+    # plain FP64, one request at a time, first come first served
+    lat, clock, done = [], 0.0, 0
+    t0 = time.perf_counter()
+    for a, k in zip(arrivals, picks):
+        now = time.perf_counter() - t0
+        if now < a:
+            time.sleep(a - now)
+        now = time.perf_counter() - t0
+        if now >= horizon:
+            break
+        r = solver.solve(pool[int(k)], tol=1e-6, iteration_limit=100000,
+                         time_limit=max(1e-3, horizon - now))
+        end = time.perf_counter() - t0
+        if end <= horizon:
+            lat.append(end - a)
+            done += 1
+    plain = summary(lat, done, horizon)
+    return {"workload": f"config5_poisson_{args.serve_rate:g}_per_s_{args.serve_seconds:g}s_"
+                        f"m500_200000", "pool": len(pool), "window_s": horizon,
+            "served_continuous_batching": served, "plain_fp64_one_at_a_time": plain}
+
+
+def synth_pool(args):
+    from niryukti_b200 import synth
+    return synth.batch_instances(count=args.serve_pool, m_lo=500, m_hi=200000, qp_frac=0.2,
+                                 seed=5)
 
 
 # ---------------------------------------------------------------- engine arm
@@ -561,9 +658,17 @@ def main():
     ap.add_argument("--batch-only", action="store_true",
                     help="print only the config-4 batched-solve section")
     ap.add_argument("--batch-count", type=int, default=512)
+    ap.add_argument("--serve", action="store_true",
+                    help="print only the config-5 served-stream section")
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--serve-seconds", type=float, default=60.0)
+    ap.add_argument("--serve-drain", type=float, default=0.0)
+    ap.add_argument("--serve-pool", type=int, default=128)
     ap.add_argument("--batch-m-hi", type=int, default=50000)
-    ap.add_argument("--batch-sample", type=int, default=6)
-    ap.add_argument("--batch-precision", default="mixed", choices=["fp64", "mixed", "fp32"])
+    ap.add_argument("--batch-sample", type=int, default=16)
+    ap.add_argument("--batch-precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--batch-cpu-sample", type=int, default=4,
+                    help="smallest sampled instances also solved by the reference on the CPU")
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per launch of the top kernel from an ncu capture")
     args = ap.parse_args()
@@ -575,6 +680,9 @@ def main():
         return solve_child(args)
     if args.batch_only:
         print(json.dumps({"batch": batch_section(args)}))
+        return
+    if args.serve:
+        print(json.dumps({"serve": serve_section(args)}))
         return
     world, rank, local = dist_setup()
     if args.impl == "reference":

@@ -246,7 +246,9 @@ nk_status nk_solve(const nk_model *model, const nk_solve_options *options,
  * boundaries.  Handles are single-threaded; nk_batch_prepare is thread-safe
  * and touches no device, so requests can be prepared while the batch runs. */
 typedef struct {
-    double tol, time_limit;   /* per instance (1e-6, 60 s from admission) */
+    double tol;               /* relative KKT tolerance of the batch (1e-6) */
+    double time_limit;        /* per instance, from admission (60 s); nk_batch_prepare
+                                 takes an instance's limits from its own options */
     int64_t iteration_limit;  /* per instance (100000) */
     int check_every;          /* trials between candidate checks (100) */
     int presolve, scaling_combined, scaling_passes, adaptive, restart, graphs;
@@ -283,6 +285,10 @@ nk_status nk_batch_result(nk_batch *batch, int64_t id, nk_solve_result *result, 
                           double *y);
 nk_status nk_batch_info(nk_batch *batch, int *active, double *used_bytes, double *budget_bytes,
                         int *variant_primal, int *variant_dual);
+/* Progress of a running (or finished, not yet collected) instance: {iterations,
+ * restarts, best KKT estimate, primal weight, step, iterations since the last
+ * restart, KKT at the last restart, 1 when in FP64}. */
+nk_status nk_batch_progress(nk_batch *batch, int64_t id, double progress[8]);
 /* Profiling (no reference counterpart): mean time of `trials` batch trials,
  * and the algorithmic bytes of one trial's two SpMV passes over all instances. */
 nk_status nk_batch_time_trials(nk_batch *batch, int trials, double *ms, int64_t *bytes_per_trial);

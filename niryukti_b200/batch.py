@@ -50,6 +50,7 @@ def _bind():
                                 C.POINTER(C.c_int)]
     L.nk_batch_time_trials.argtypes = [P, C.c_int, _D, _I]
     L.nk_batch_kernel_times.argtypes = [P, _D, _D]
+    L.nk_batch_progress.argtypes = [P, C.c_int64, _D]
     L._nk_batch_bound = True
     return L
 
@@ -129,10 +130,15 @@ class BatchEngine:
 
     def prepare(self, model) -> PreparedInstance:
         """Thread-safe: presolve, scaling, start-point checks, layout."""
+        return self.prepare_with(model, self.options)
+
+    def prepare_with(self, model, options: NkBatchOptions) -> PreparedInstance:
+        """prepare() with an instance's own limits (iteration and time limit;
+        the tolerance and precision must be the batch's)."""
         view = _ModelView(model)
         h = C.c_void_p()
         b = C.c_double()
-        check(self._L.nk_batch_prepare(C.byref(view.s), C.byref(self.options), C.byref(h),
+        check(self._L.nk_batch_prepare(C.byref(view.s), C.byref(options), C.byref(h),
                                        C.byref(b)))
         return PreparedInstance(h, int(model.n), int(model.m), b.value)
 
@@ -169,6 +175,13 @@ class BatchEngine:
                     "threads": (128, 256, 512)[v % 3]}
         return {"active": a.value, "used_bytes": u.value, "budget_bytes": b.value,
                 "primal_variant": variant(vp.value), "dual_variant": variant(vd.value)}
+
+    def progress(self, ident: int) -> dict:
+        v = np.zeros(8)
+        check(self._L.nk_batch_progress(self._h, int(ident), v.ctypes.data_as(_D)))
+        keys = ("iterations", "restarts", "best_kkt", "weight", "step", "since_restart",
+                "restart_kkt", "fp64")
+        return dict(zip(keys, v.tolist()))
 
     def kernel_times(self):
         """The autotuner's best primal and dual kernel times (ms)."""

@@ -53,6 +53,8 @@ struct BatchItem {
     double step = 1, weight = 1, a_norm = 0, q_norm = 0;
     bool sparse_q = false;
     size_t bytes = 0;
+    int64_t iteration_limit = 100000; // this instance's limits (from its prepare options)
+    double time_limit = 60;
 };
 
 namespace batch_detail {
@@ -99,6 +101,8 @@ inline std::unique_ptr<BatchItem> batch_prepare(const HostModel &original, const
     using namespace batch_detail;
     auto it = std::make_unique<BatchItem>();
     BatchItem &B = *it;
+    B.iteration_limit = o.iteration_limit;
+    B.time_limit = o.time_limit;
     auto t0 = SteadyClock::now();
     B.orig = original;
     B.verifier = std::make_unique<Verifier>(B.orig);
@@ -436,6 +440,19 @@ class Batch {
                 break;
         }
         return done;
+    }
+
+    // Progress of an instance: iterations, restarts, best KKT estimate, primal
+    // weight, step, iterations since restart, KKT at the last restart, phase.
+    void progress(int64_t id, double *out) const {
+        auto f = by_id_.find(id);
+        if (f == by_id_.end())
+            throw Error(NK_ERR_INVALID, "unknown batch instance id");
+        const Slot &S = slots_[size_t(f->second)];
+        const double v[8] = {double(S.iterations), double(S.restarts), S.best.kkt, S.weight,
+                             S.step, double(S.since_restart), S.restart_kkt,
+                             S.fp64_phase ? 1. : 0.};
+        std::memcpy(out, v, sizeof(v));
     }
 
     // Result of a finished instance; frees its slot.
@@ -1166,11 +1183,11 @@ class Batch {
                     continue;
                 }
             }
-            if (S.iterations >= o_.iteration_limit) {
+            if (S.iterations >= B.iteration_limit) {
                 retire(S, NK_SOLVE_ITERATION_LIMIT);
                 continue;
             }
-            if (since(S.start) >= o_.time_limit) {
+            if (since(S.start) >= B.time_limit) {
                 retire(S, NK_SOLVE_TIME_LIMIT);
                 continue;
             }

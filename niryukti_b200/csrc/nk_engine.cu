@@ -1851,6 +1851,13 @@ nk_status nk_batch_info(nk_batch *h, int *active, double *used_bytes, double *bu
     });
 }
 
+nk_status nk_batch_progress(nk_batch *h, int64_t id, double progress[8]) {
+    return guard([&] {
+        if (!h || !progress)
+            throw nk::Error(NK_ERR_INVALID, "null argument");
+        h->b.progress(id, progress);
+    });
+}
 nk_status nk_batch_kernel_times(nk_batch *h, double *primal_ms, double *dual_ms) {
     return guard([&] {
         if (!h || !primal_ms || !dual_ms)
