@@ -408,6 +408,32 @@ def batch_section(args):
     return out
 
 
+def batch_throughput(args):
+    """Trial throughput of the config-4 batch (no solve): admit every
+    instance, run one check interval (this also autotunes the kernels), then
+    time --batch-trials PDHG trials of the whole batch with CUDA events."""
+    from concurrent.futures import ThreadPoolExecutor
+    from niryukti_b200 import batch as nb
+    models = batch_models(args)
+    with nb.BatchEngine(matrix_precision=args.batch_precision, iteration_limit=10**9,
+                        time_limit=1e9) as eng:
+        with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as pool:
+            items = list(pool.map(eng.prepare, models))
+        for k, it in enumerate(items):
+            if not eng.admit(it, k):
+                raise MemoryError("config-4 batch does not fit the device budget")
+        eng.step(1)
+        ms, bts = eng.time_trials(args.batch_trials)
+        kp, kd = eng.kernel_times()
+        info = eng.info()
+    per = ms / max(1, args.batch_trials)
+    return {"workload": f"config4_{len(models)}_uneven_lp_qp", "precision": args.batch_precision,
+            "trials": args.batch_trials, "ms_per_trial": per,
+            "spmv_bytes_per_trial": bts, "spmv_GBps": bts / per / 1e6,
+            "tuned_kernel_ms": {"batch_primal": kp, "batch_dual": kd},
+            "variants": {"primal": info["primal_variant"], "dual": info["dual_variant"]}}
+
+
 # ---------------------------------------------------------------- serving (config 5)
 def serve_section(args):
     """Config 5: Poisson arrivals at --serve-rate requests/s for --serve-seconds,
@@ -440,7 +466,8 @@ def serve_section(args):
     # served: a feeder submits at the arrival times
     svc = serve.SolveService(memory_budget=150e9, matrix_precision="mixed",
                              prepare_workers=os.cpu_count() or 8,
-                             iteration_limit=100000, time_limit=horizon)
+                             iteration_limit=100000, time_limit=horizon,
+                             max_active_nnz=int(args.serve_active_nnz))
     lat, statuses = [], {}
     futs = []
     t0 = time.perf_counter()
@@ -658,12 +685,16 @@ def main():
     ap.add_argument("--batch-only", action="store_true",
                     help="print only the config-4 batched-solve section")
     ap.add_argument("--batch-count", type=int, default=512)
+    ap.add_argument("--batch-trials", type=int, default=0,
+                    help="with --batch-only: time this many batch trials instead of solving")
     ap.add_argument("--serve", action="store_true",
                     help="print only the config-5 served-stream section")
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-seconds", type=float, default=60.0)
-    ap.add_argument("--serve-drain", type=float, default=0.0)
-    ap.add_argument("--serve-pool", type=int, default=128)
+    ap.add_argument("--serve-drain", type=float, default=60.0)
+    ap.add_argument("--serve-pool", type=int, default=64)
+    ap.add_argument("--serve-active-nnz", type=float, default=16e6,
+                    help="work cap of the running batch (nonzeros)")
     ap.add_argument("--batch-m-hi", type=int, default=50000)
     ap.add_argument("--batch-sample", type=int, default=16)
     ap.add_argument("--batch-precision", default="mixed", choices=["fp64", "mixed"])
@@ -679,7 +710,8 @@ def main():
     if args.solve_child:
         return solve_child(args)
     if args.batch_only:
-        print(json.dumps({"batch": batch_section(args)}))
+        print(json.dumps({"batch": batch_throughput(args) if args.batch_trials
+                          else batch_section(args)}))
         return
     if args.serve:
         print(json.dumps({"serve": serve_section(args)}))

@@ -192,12 +192,13 @@ class SolveService:
 
     def __init__(self, *, memory_budget=150e9, matrix_precision="mixed", tol=1e-6,
                  iteration_limit=100000, time_limit=600.0, check_every=100,
-                 prepare_workers=8, autotune=True, max_active_nnz=200_000_000):
+                 prepare_workers=8, autotune=True, max_active_nnz=16_000_000):
         """memory_budget: device bytes for resident instances (admission by
         footprint).  max_active_nnz: work cap of the running batch (nonzeros
-        of A and Q over the admitted instances); it bounds the time of one
-        batch trial, so that admitted instances keep a useful iteration rate
-        when the offered load exceeds the GPU's capacity."""
+        of A and Q over the admitted instances).  A batch trial over 16 M
+        nonzeros already keeps the GPU's memory system busy (about 0.2 ms per
+        trial); admitting more work makes every trial longer without raising
+        throughput, so admitted instances would only finish later."""
         self.tol = tol
         self.max_active_nnz = max_active_nnz
         self._active_nnz = 0
