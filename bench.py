@@ -579,8 +579,16 @@ def engine_arm(args, world, rank, local):
     if pk.exists():
         peaks = json.loads(pk.read_text())
     peak = float(peaks.get("hbm_gbs", 6650.0))
+    traffic, traffic_source = args.traffic, "--traffic" if args.traffic else None
+    if traffic is None and args.precision == "fp64" and not args.small and args.scale == 1.0:
+        # DRAM bytes per launch from the ncu capture of the config-2 shape at half
+        # size (profiles/fused_pdhg_kernels_config2_scaled_half.md: read + write),
+        # scaled by 2: every unit (nonzeros, rows, columns) doubles
+        traffic = {"primal_kernel": 2 * 183.26e6, "dual_kernel": 2 * 166.60e6}[top]
+        traffic_source = "ncu dram__bytes_read.sum + dram__bytes_write.sum at scale 0.5, x2"
     roofline = {"bound": "hbm", "kernel": top, "achieved": kernels[top]["GBps"], "peak": peak,
-                "unit": "GB/s", "frac": kernels[top]["GBps"] / peak, "traffic": args.traffic,
+                "unit": "GB/s", "frac": kernels[top]["GBps"] / peak, "traffic": traffic,
+                "traffic_source": traffic_source,
                 "peak_source": "measured" if pk.exists() else "fallback"}
 
     # e2e through the C ABI with host buffers: per step upload (x, y), 100 trials,
