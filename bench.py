@@ -353,6 +353,7 @@ def batch_section(args):
                 results[k] = eng.result(k)
                 finish_t[k] = time.perf_counter() - g0
         gpu_s = time.perf_counter() - g0
+        phases = eng.phase_seconds()
     statuses = {}
     for r in results.values():
         statuses[r["status"]] = statuses.get(r["status"], 0) + 1
@@ -383,6 +384,7 @@ def batch_section(args):
            "solves_per_s": len(models) / gpu_s,
            "solves_per_s_with_prepare": len(models) / (gpu_s + prep_s),
            "kernel_variants": {"primal": info["primal_variant"], "dual": info["dual_variant"]},
+           "check_interval_seconds": phases,
            "plain_fp64_one_by_one": {"sample": plain, "extrapolated_s": plain_s,
                                      "solves_per_s": len(models) / plain_s},
            "speedup_vs_plain": plain_s / gpu_s,

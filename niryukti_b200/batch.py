@@ -51,6 +51,7 @@ def _bind():
     L.nk_batch_time_trials.argtypes = [P, C.c_int, _D, _I]
     L.nk_batch_kernel_times.argtypes = [P, _D, _D]
     L.nk_batch_progress.argtypes = [P, C.c_int64, _D]
+    L.nk_batch_phase_seconds.argtypes = [P, _D]
     L._nk_batch_bound = True
     return L
 
@@ -182,6 +183,12 @@ class BatchEngine:
         keys = ("iterations", "restarts", "best_kkt", "weight", "step", "since_restart",
                 "restart_kkt", "fp64")
         return dict(zip(keys, v.tolist()))
+
+    def phase_seconds(self) -> dict:
+        v = np.zeros(6)
+        check(self._L.nk_batch_phase_seconds(self._h, v.ctypes.data_as(_D)))
+        return dict(zip(("controls", "trials", "evaluation", "driver", "restarts", "close"),
+                        v.tolist()))
 
     def kernel_times(self):
         """The autotuner's best primal and dual kernel times (ms)."""

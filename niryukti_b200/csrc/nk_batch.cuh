@@ -52,6 +52,7 @@ struct BatchItem {
     double os = 1, cscale = 1, offset_o = 0, offset_s = 0, cfixed = 0;
     double step = 1, weight = 1, a_norm = 0, q_norm = 0;
     bool sparse_q = false;
+    bool is_qp = false; // the caller's model has quadratic terms (cached: O(n) to test)
     size_t bytes = 0;
     int64_t iteration_limit = 100000; // this instance's limits (from its prepare options)
     double time_limit = 60;
@@ -105,6 +106,7 @@ inline std::unique_ptr<BatchItem> batch_prepare(const HostModel &original, const
     B.time_limit = o.time_limit;
     auto t0 = SteadyClock::now();
     B.orig = original;
+    B.is_qp = B.orig.is_qp();
     B.verifier = std::make_unique<Verifier>(B.orig);
     B.prep = prepare(B.orig, o.prepare);
     SolveReport &R = B.report;
@@ -366,6 +368,7 @@ class Batch {
     int active() const { return int(order_.size()) + int(joining_.size()); }
     int variant_primal() const { return vp_; }
     double tuned_ms_primal() const { return ms_primal_; }
+    const double *phase_seconds() const { return phase_; }
     double tuned_ms_dual() const { return ms_dual_; }
     int variant_dual() const { return vd_; }
 
@@ -546,6 +549,10 @@ class Batch {
     bool dirty_ = true, tuned_ = false;
     int vp_ = 13, vd_ = 13; // kernel variants (autotuned, see launch_half)
     float ms_primal_ = 0, ms_dual_ = 0; // their best times when tuned
+    // wall seconds per part of a check interval: control upload, trials,
+    // candidate evaluation, per-instance driver logic (host), best/restart
+    // kernels, closing certification of finished instances
+    double phase_[6] = {};
     int tuned_chunks_ = 0;
     cudaGraphExec_t graph_ = nullptr;
 
@@ -606,6 +613,8 @@ class Batch {
         // 20 column vectors
         d.c = cvec(B.c);
         d.q = cvec(B.q);
+        if (std::all_of(B.q.begin(), B.q.end(), [](double v) { return v == 0; }))
+            d.q = nullptr; // an LP: the kernels skip the diagonal's loads
         d.lb = cvec(B.lb);
         d.ub = cvec(B.ub);
         d.x[0] = cvec(B.x0);
@@ -967,7 +976,7 @@ class Batch {
             a.gap = std::max(a.gap, std::abs(a.objective - a.lower_bound) /
                                         (1 + std::abs(a.objective) + std::abs(a.lower_bound)));
         }
-        if (!B.orig.is_qp())
+        if (!B.is_qp)
             a.lower_bound = -kInf;
         a.kkt = std::max({a.primal, a.dual, a.gap});
         a.finite = std::isfinite(a.objective) && std::isfinite(a.kkt) && std::isfinite(a.gap) &&
@@ -1069,7 +1078,9 @@ class Batch {
 
     // One check interval for every listed instance.
     void run_interval() {
+        auto tp = SteadyClock::now();
         push_steps();
+        phase_[0] += since(tp);
         auto t0 = SteadyClock::now();
         if (o_.graphs)
             cuda_check(cudaGraphLaunch(graph(), stream_), "graph launch");
@@ -1078,6 +1089,7 @@ class Batch {
                 launch_trial(vp_, vd_);
         sync_progress(true);
         const double dt = since(t0);
+        phase_[1] += dt;
         auto t1 = SteadyClock::now();
         const int n = int(order_.size());
         // fold pending averages, then evaluate current (slot 0) and average (slot 1)
@@ -1094,6 +1106,8 @@ class Batch {
                                    cudaMemcpyDeviceToHost, stream_), "controls");
         cuda_check(cudaStreamSynchronize(stream_), "evaluation");
         const double de = since(t1);
+        phase_[2] += de;
+        auto t2h = SteadyClock::now();
         std::vector<int> keep_on, keep_src, restart_on, restart_src, refine_on;
         const double phase_tol = o_.phase_tol > 0 ? o_.phase_tol : 10 * o_.tol;
         std::vector<Accuracy> chosen(static_cast<size_t>(n));
@@ -1154,7 +1168,8 @@ class Batch {
                 bool found = false;
                 for (int r = 0; r < 2 && !found; ++r) {
                     const double *sv = r ? other_ray : ray;
-                    if (!(sv[10] == 0 && sv[11] + sv[12] > -1e-9 * (1 + sv[13])))
+                    // as in the single driver: only a bound that may be positive
+                    if (!(sv[10] == 0 && sv[11] + sv[12] + 1e-9 * sv[13] > 0))
                         continue;
                     auto t2 = SteadyClock::now();
                     std::vector<double> ox, oy;
@@ -1212,6 +1227,8 @@ class Batch {
                 restart_src.push_back(src);
             }
         }
+        phase_[3] += since(t2h);
+        auto t3 = SteadyClock::now();
         // best points (before any restart moves the iterate)
         if (!keep_on.empty()) {
             set_mask(keep_on, keep_src);
@@ -1282,9 +1299,12 @@ class Batch {
             cuda_check(cudaGetLastError(), "batch restart");
         }
         cuda_check(cudaStreamSynchronize(stream_), "interval");
+        phase_[4] += since(t3);
+        auto t4 = SteadyClock::now();
         for (int b : order_)
             if (slots_[size_t(b)].finished)
                 close(slots_[size_t(b)]);
+        phase_[5] += since(t4);
     }
 };
 

@@ -30,7 +30,7 @@ struct BInst {
     const int32_t *q_idx;
     const float *q_val;
     const double *q_val64;
-    const double *c, *q, *lb, *ub, *rl, *ru;
+    const double *c, *q, *lb, *ub, *rl, *ru; // q: null when the diagonal is all zero
     double *x[2], *y[2], *ax[2], *xa, *ya, *dx;
     // evaluation: original-space constants and work vectors
     const double *cs, *olb, *oub, *rs, *shift, *orl, *oru;
@@ -157,7 +157,8 @@ __global__ void batch_primal(const BInst *__restrict__ ins, const BCtl *__restri
             const double qa = sq ? chunk_q(I, f64, j, valid, x) : 0.;
             double mine = 0;
             if (valid) {
-                const double xj = x[j], cj = I.c[j], qj = I.q[j], lj = I.lb[j], uj = I.ub[j];
+                const double xj = x[j], cj = I.c[j], qj = I.q ? I.q[j] : 0., lj = I.lb[j],
+                             uj = I.ub[j];
                 const double aj = pending ? I.xa[j] : 0.;
                 // FP64 accumulation starts from c_j, like the CPU loop (src/cpu.cpp:108-111)
                 double g = inst_dot<U>(f64, I.t_cptr, I.t_idx, I.t_val, I.t_val64, j, I.t_len[j],
@@ -389,9 +390,10 @@ __global__ void batch_kkt(const BInst *ins, const BCtl *ctl, const int *mask, in
                 const double qxs = I.q_ptr ? I.e_qx[e] : 0.;
                 const double aty = I.e_aty[slot][e];
                 const double lin = (I.c[e] + aty) * f;
-                const double curv = (I.q[e] * xs + qxs) * f;
+                const double qe = I.q ? I.q[e] : 0.;
+                const double curv = (qe * xs + qxs) * f;
                 const double g = lin + curv;
-                v[4] = I.c[e] * xs + .5 * I.q[e] * xs * xs + .5 * xs * qxs;
+                v[4] = I.c[e] * xs + .5 * qe * xs * xs + .5 * xs * qxs;
                 if (!isfinite(lin) || !isfinite(g) || !isfinite(xo))
                     v[9] = 1;
                 const double d = clampd(g, xo - hi, xo - lo);
@@ -409,7 +411,7 @@ __global__ void batch_kkt(const BInst *ins, const BCtl *ctl, const int *mask, in
                     else
                         v[7] = g * arg - curv * xo / 2;
                 } else {
-                    const double qo = I.q[e] * f / cj;
+                    const double qo = qe * f / cj;
                     arg = qo > 0 ? clampd(-lin / qo, lo, hi) : lin > 0 ? lo : lin < 0 ? hi
                                                                                     : clampd(0., lo, hi);
                     if (!isfinite(arg))

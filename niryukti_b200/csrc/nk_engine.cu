@@ -1858,6 +1858,13 @@ nk_status nk_batch_progress(nk_batch *h, int64_t id, double progress[8]) {
         h->b.progress(id, progress);
     });
 }
+nk_status nk_batch_phase_seconds(nk_batch *h, double seconds[6]) {
+    return guard([&] {
+        if (!h || !seconds)
+            throw nk::Error(NK_ERR_INVALID, "null argument");
+        std::memcpy(seconds, h->b.phase_seconds(), 6 * sizeof(double));
+    });
+}
 nk_status nk_batch_kernel_times(nk_batch *h, double *primal_ms, double *dual_ms) {
     return guard([&] {
         if (!h || !primal_ms || !dual_ms)

@@ -277,6 +277,7 @@ struct DeviceSolve {
                                 // 3 rays x kRayValues
     int grid = 148;
     double os = 1, cscale = 1, offset_o = 0, offset_s = 0, cfixed = 0;
+    bool orig_is_qp = false; // the caller's model has quadratic terms (cached: O(n) to test)
     std::vector<int64_t> cperm, rperm; // engine position -> prepared index
 
     DeviceSolve(const Prepared &p, const HostModel &o) : prep(p), orig(o) {}
@@ -310,6 +311,7 @@ struct DeviceSolve {
             cuda_check(cudaMemcpy(rperm.data(), E->row_perm.p, size_t(m) * 8, cudaMemcpyDeviceToHost),
                        "row order");
         // constants of the original-space evaluation
+        orig_is_qp = orig.is_qp();
         os = prep.objective_scale;
         offset_o = orig.offset;
         offset_s = pm.offset;
@@ -458,8 +460,9 @@ struct DeviceSolve {
         for (int r = 0; r < 3; ++r) {
             const double *v = host_out + kRayOut + r * kRayValues;
             // FP64 sums of the bound's terms err by far less than 1e-9 of their
-            // magnitude: below that margin the exact bound is negative too
-            ok[size_t(r)] = v[0] == 0 && v[1] + v[2] > -1e-9 * (1 + v[3]);
+            // magnitude: at or below that margin the exact bound cannot be
+            // positive (a zero ray has bound 0 and magnitude 0)
+            ok[size_t(r)] = v[0] == 0 && v[1] + v[2] + 1e-9 * v[3] > 0;
         }
         return ok;
     }
@@ -491,7 +494,7 @@ struct DeviceSolve {
             a.gap = std::max(a.gap, std::abs(a.objective - a.lower_bound) /
                                         (1 + std::abs(a.objective) + std::abs(a.lower_bound)));
         }
-        if (!orig.is_qp())
+        if (!orig_is_qp)
             a.lower_bound = -kInf;
         a.kkt = std::max({a.primal, a.dual, a.gap});
         a.finite = std::isfinite(a.objective) && std::isfinite(a.kkt) && std::isfinite(a.gap) &&
