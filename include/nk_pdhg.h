@@ -297,9 +297,10 @@ nk_status nk_batch_time_trials(nk_batch *batch, int trials, double *ms, int64_t 
 nk_status nk_batch_kernel_times(nk_batch *batch, double *primal_ms, double *dual_ms);
 /* Profiling (no reference counterpart): wall seconds spent so far in the parts
  * of the check intervals: control upload, trials, candidate evaluation,
- * per-instance driver logic on the host, best-point/restart kernels, closing
- * certification of finished instances. */
-nk_status nk_batch_phase_seconds(nk_batch *batch, double seconds[6]);
+ * per-instance driver logic on the host (with certification), best-point and
+ * restart kernels, closing certification of finished instances, and work-list
+ * rebuilds (including kernel tuning and graph capture). */
+nk_status nk_batch_phase_seconds(nk_batch *batch, double seconds[7]);
 
 /* KKT proxy without any device allocation.  No counterpart in the reference:
  * it exists for callers that must not allocate device memory themselves --

@@ -185,10 +185,10 @@ class BatchEngine:
         return dict(zip(keys, v.tolist()))
 
     def phase_seconds(self) -> dict:
-        v = np.zeros(6)
+        v = np.zeros(7)
         check(self._L.nk_batch_phase_seconds(self._h, v.ctypes.data_as(_D)))
-        return dict(zip(("controls", "trials", "evaluation", "driver", "restarts", "close"),
-                        v.tolist()))
+        return dict(zip(("controls", "trials", "evaluation", "driver", "restarts", "close",
+                         "lists"), v.tolist()))
 
     def kernel_times(self):
         """The autotuner's best primal and dual kernel times (ms)."""

@@ -56,9 +56,30 @@ struct BatchItem {
     size_t bytes = 0;
     int64_t iteration_limit = 100000; // this instance's limits (from its prepare options)
     double time_limit = 60;
+    std::vector<int64_t> col_cost, row_cost; // estimated work per SELL chunk (work lists)
 };
 
 namespace batch_detail {
+
+// Runs f(0 .. count-1) on up to hardware_concurrency host threads.
+template <class F> void parallel_for(size_t count, F &&f) {
+    const size_t threads = std::min<size_t>(count, std::max(1u, std::thread::hardware_concurrency()));
+    if (threads <= 1) {
+        for (size_t k = 0; k < count; ++k)
+            f(k);
+        return;
+    }
+    std::atomic<size_t> next{0};
+    std::vector<std::thread> pool;
+    for (size_t t = 0; t < threads; ++t)
+        pool.emplace_back([&]() {
+            host_serial(true); // the workers are the parallelism: no nested OpenMP teams
+            for (size_t k; (k = next.fetch_add(1)) < count;)
+                f(k);
+        });
+    for (auto &th : pool)
+        th.join();
+}
 
 // SELL-32 of the rows of a CSR (ptr/index/value in prepared order) taken in
 // engine order `perm`, column indices mapped through `inv`.
@@ -205,6 +226,25 @@ inline std::unique_ptr<BatchItem> batch_prepare(const HostModel &original, const
         }
         B.q_norm = std::nextafter(double(largest), INFINITY);
     }
+    // estimated work per chunk for the work lists: the chunk's SELL width plus
+    // its Q work (rows longer than 32 are shared by the warp, 32 entries a step)
+    for (int64_t c = 0; c < (B.n + 31) / 32; ++c) {
+        int64_t cost = (B.t_cptr[size_t(c + 1)] - B.t_cptr[size_t(c)]) / 32 + 4;
+        if (B.sparse_q) {
+            int64_t lane_max = 0, shared = 0;
+            for (int64_t j = c * 32; j < std::min<int64_t>(B.n, c * 32 + 32); ++j) {
+                const int64_t len = B.q_ptr[size_t(j + 1)] - B.q_ptr[size_t(j)];
+                if (len > 32)
+                    shared += (len + 31) / 32;
+                else
+                    lane_max = std::max(lane_max, len);
+            }
+            cost += lane_max + shared;
+        }
+        B.col_cost.push_back(cost);
+    }
+    for (int64_t c = 0; c < (B.m + 31) / 32; ++c)
+        B.row_cost.push_back((B.a_cptr[size_t(c + 1)] - B.a_cptr[size_t(c)]) / 32 + 4);
     auto by_col = [&](const std::vector<double> &v) {
         std::vector<double> out(size_t(B.n));
         for (int64_t j = 0; j < B.n; ++j)
@@ -430,7 +470,9 @@ class Batch {
                 reported_.insert(id);
             }
         for (int c = 0; c < checks; ++c) {
+            auto tl = SteadyClock::now();
             rebuild_lists();
+            phase_[6] += since(tl);
             if (order_.empty())
                 break;
             run_interval();
@@ -552,7 +594,7 @@ class Batch {
     // wall seconds per part of a check interval: control upload, trials,
     // candidate evaluation, per-instance driver logic (host), best/restart
     // kernels, closing certification of finished instances
-    double phase_[6] = {};
+    double phase_[7] = {}; // ... and work-list rebuilds (with tuning and graph capture)
     int tuned_chunks_ = 0;
     cudaGraphExec_t graph_ = nullptr;
 
@@ -681,6 +723,12 @@ class Batch {
     }
 
     // ---------------------------------------------------------------- lists
+    // Device buffers of the work lists only grow: a shrinking batch reuses them.
+    template <class T> static void ensure(DevBuf<T> &d, size_t count) {
+        if (d.n < count)
+            d.alloc(count + count / 4);
+    }
+
     void rebuild_lists() {
         if (!joining_.empty()) {
             for (int b : joining_)
@@ -706,27 +754,13 @@ class Batch {
             const BatchItem &B = *slots_[size_t(b)].item;
             cf.push_back(int(cols.size()));
             for (int64_t c = 0; c < (B.n + 31) / 32; ++c) {
-                // cost: the chunk's SELL width plus its Q work (long rows are
-                // shared by the warp, 32 entries per step)
-                int64_t cost = (B.t_cptr[size_t(c + 1)] - B.t_cptr[size_t(c)]) / 32 + 4;
-                if (B.sparse_q) {
-                    int64_t lane_max = 0, shared = 0;
-                    for (int64_t j = c * 32; j < std::min<int64_t>(B.n, c * 32 + 32); ++j) {
-                        const int64_t len = B.q_ptr[size_t(j + 1)] - B.q_ptr[size_t(j)];
-                        if (len > 32)
-                            shared += (len + 31) / 32;
-                        else
-                            lane_max = std::max(lane_max, len);
-                    }
-                    cost += lane_max + shared;
-                }
-                ccost.push_back(cost);
+                ccost.push_back(B.col_cost[size_t(c)]);
                 cols.push_back(make_int2(b, int(c)));
             }
             cc.push_back(int(cols.size()) - cf.back());
             rf.push_back(int(rows.size()));
             for (int64_t c = 0; c < (B.m + 31) / 32; ++c) {
-                rcost.push_back((B.a_cptr[size_t(c + 1)] - B.a_cptr[size_t(c)]) / 32 + 4);
+                rcost.push_back(B.row_cost[size_t(c)]);
                 rows.push_back(make_int2(b, int(c)));
             }
             rc.push_back(int(rows.size()) - rf.back());
@@ -738,7 +772,10 @@ class Batch {
         // round-robin gives every warp a similar share (longest-first greedy)
         auto runs = [&](const std::vector<int2> &list, const std::vector<int64_t> &cost,
                         const std::vector<int> &first, const std::vector<int> &count, int K) {
-            std::vector<std::pair<int64_t, BWork>> items;
+            // items with their costs, then a stable counting sort, costliest first
+            std::vector<BWork> items;
+            std::vector<int64_t> icost;
+            int64_t top = 0;
             for (size_t k = 0; k < first.size(); ++k)
                 for (int c = 0; c < count[k]; c += K) {
                     const int len = std::min(K, count[k] - c);
@@ -746,33 +783,44 @@ class Batch {
                     for (int t = 0; t < len; ++t)
                         total += cost[size_t(first[k] + c + t)];
                     const int2 head = list[size_t(first[k] + c)];
-                    items.push_back({total, BWork{head.x, head.y, first[k] + c, len}});
+                    items.push_back(BWork{head.x, head.y, first[k] + c, len});
+                    icost.push_back(total);
+                    top = std::max(top, total);
                 }
-            std::stable_sort(items.begin(), items.end(),
-                             [](const auto &a, const auto &b) { return a.first > b.first; });
-            std::vector<BWork> out;
-            for (auto &p : items)
-                out.push_back(p.second);
+            std::vector<int64_t> start(size_t(top + 2), 0);
+            for (int64_t c : icost)
+                ++start[size_t(top - c + 1)];
+            for (size_t b = 1; b < start.size(); ++b)
+                start[b] += start[b - 1];
+            std::vector<BWork> out(items.size());
+            for (size_t k = 0; k < items.size(); ++k)
+                out[size_t(start[size_t(top - icost[k])]++)] = items[k];
             return out;
         };
+        auto upload_list = [&](DevBuf<BWork> &d, const std::vector<BWork> &h) {
+            ensure(d, std::max<size_t>(1, h.size()));
+            if (!h.empty())
+                cuda_check(cudaMemcpy(d.p, h.data(), h.size() * sizeof(BWork), cudaMemcpyHostToDevice),
+                           "lists");
+        };
         for (int r = 0; r < kRunLengths; ++r) {
-            auto wc = runs(cols, ccost, cf, cc, kRunLength[r]);
-            auto wr = runs(rows, rcost, rf, rc, kRunLength[r]);
-            nwc_[r] = int(wc.size());
-            nwr_[r] = int(wr.size());
-            d_wcols_[r].alloc(std::max<size_t>(1, wc.size()));
-            d_wrows_[r].alloc(std::max<size_t>(1, wr.size()));
-            if (!wc.empty())
-                cuda_check(cudaMemcpy(d_wcols_[r].p, wc.data(), wc.size() * sizeof(BWork),
-                                      cudaMemcpyHostToDevice), "lists");
-            if (!wr.empty())
-                cuda_check(cudaMemcpy(d_wrows_[r].p, wr.data(), wr.size() * sizeof(BWork),
-                                      cudaMemcpyHostToDevice), "lists");
+            // after tuning only the chosen run lengths are launched
+            const bool need_c = !tuned_ || r == vp_ / 9, need_r = !tuned_ || r == vd_ / 9;
+            if (need_c) {
+                auto wc = runs(cols, ccost, cf, cc, kRunLength[r]);
+                nwc_[r] = int(wc.size());
+                upload_list(d_wcols_[r], wc);
+            }
+            if (need_r) {
+                auto wr = runs(rows, rcost, rf, rc, kRunLength[r]);
+                nwr_[r] = int(wr.size());
+                upload_list(d_wrows_[r], wr);
+            }
         }
         ncols_ = int(cols.size());
         nrows_ = int(rows.size());
         auto up = [&](auto &d, const auto &h) {
-            d.alloc(std::max<size_t>(1, h.size()));
+            ensure(d, std::max<size_t>(1, h.size()));
             if (!h.empty())
                 cuda_check(cudaMemcpy(d.p, h.data(), h.size() * sizeof(h[0]), cudaMemcpyHostToDevice),
                            "lists");
@@ -784,10 +832,10 @@ class Batch {
         up(d_cc_, cc);
         up(d_rf_, rf);
         up(d_rc_, rc);
-        d_pp_.alloc(size_t(std::max(1, ncols_)));
-        d_pd_.alloc(size_t(std::max(1, 2 * nrows_)));
-        d_pk_.alloc(size_t(std::max(1, ncols_ + nrows_)) * kBatchKkt);
-        d_out_.alloc(size_t(std::max<size_t>(1, order_.size())) * kBatchKkt * 2);
+        ensure(d_pp_, size_t(std::max(1, ncols_)));
+        ensure(d_pd_, size_t(std::max(1, 2 * nrows_)));
+        ensure(d_pk_, size_t(std::max(1, ncols_ + nrows_)) * kBatchKkt);
+        ensure(d_out_, size_t(std::max<size_t>(1, order_.size())) * kBatchKkt * 2);
         const size_t need = std::max<size_t>(1, order_.size()) * kBatchKkt * 2;
         if (h_out_n_ < need) {
             if (h_out_)
@@ -1056,23 +1104,39 @@ class Batch {
         dirty_ = true;
     }
 
-    // The closing evaluation of solve_continuous: certify the best point.
-    void close(Slot &S) {
-        SolveReport &R = S.item->report;
-        if (S.status == NK_SOLVE_OPTIMAL || S.status == NK_SOLVE_INFEASIBLE)
+    // The closing evaluation of solve_continuous for every instance that
+    // finished without a certificate: host copies of the best points, then the
+    // verifier on host threads.
+    void close_finished() {
+        std::vector<int> todo;
+        for (int b : order_) {
+            const Slot &S = slots_[size_t(b)];
+            const SolveReport &R = S.item->report;
+            if (S.finished && S.status != NK_SOLVE_OPTIMAL && S.status != NK_SOLVE_INFEASIBLE &&
+                S.best.finite && S.best.kkt < R.accuracy.kkt)
+                todo.push_back(b);
+        }
+        if (todo.empty())
             return;
-        if (S.best.finite && S.best.kkt < R.accuracy.kkt) {
-            auto t0 = SteadyClock::now();
-            std::vector<double> ox, oy;
-            host_point(S, S.d.best_x, S.d.best_y, ox, oy);
-            Accuracy h = S.item->verifier->evaluate(ox, oy, true);
+        const size_t nc = todo.size();
+        std::vector<std::vector<double>> ox(nc), oy(nc);
+        std::vector<Accuracy> acc(nc);
+        for (size_t k = 0; k < nc; ++k) {
+            Slot &S = slots_[size_t(todo[k])];
+            host_point(S, S.d.best_x, S.d.best_y, ox[k], oy[k]);
+        }
+        batch_detail::parallel_for(nc, [&](size_t k) {
+            acc[k] = slots_[size_t(todo[k])].item->verifier->evaluate(ox[k], oy[k], true);
+        });
+        for (size_t k = 0; k < nc; ++k) {
+            Slot &S = slots_[size_t(todo[k])];
+            SolveReport &R = S.item->report;
             S.host_checks++;
-            if (h.finite && (h.kkt < R.accuracy.kkt || !R.accuracy.finite)) {
-                R.x = std::move(ox);
-                R.y = std::move(oy);
-                R.accuracy = h;
+            if (acc[k].finite && (acc[k].kkt < R.accuracy.kkt || !R.accuracy.finite)) {
+                R.x = std::move(ox[k]);
+                R.y = std::move(oy[k]);
+                R.accuracy = acc[k];
             }
-            S.verification_seconds += since(t0);
         }
     }
 
@@ -1109,6 +1173,7 @@ class Batch {
         phase_[2] += de;
         auto t2h = SteadyClock::now();
         std::vector<int> keep_on, keep_src, restart_on, restart_src, refine_on;
+        std::vector<std::pair<int, int>> certify; // (slot, candidate) for the host verifier
         const double phase_tol = o_.phase_tol > 0 ? o_.phase_tol : 10 * o_.tol;
         std::vector<Accuracy> chosen(static_cast<size_t>(n));
         for (int k = 0; k < n; ++k) {
@@ -1147,19 +1212,9 @@ class Batch {
                 continue;
             }
             if (ca.kkt <= o_.tol && S.iterations >= S.next_host_check) {
-                auto t2 = SteadyClock::now();
-                std::vector<double> ox, oy;
-                host_point(S, point_x(S, src), point_y(S, src), ox, oy);
-                Accuracy h = B.verifier->evaluate(ox, oy, true);
-                S.host_checks++;
-                S.verification_seconds += since(t2);
-                if (h.kkt <= o_.tol) {
-                    S.item->report.x = std::move(ox);
-                    S.item->report.y = std::move(oy);
-                    S.item->report.accuracy = h;
-                    retire(S, NK_SOLVE_OPTIMAL);
-                    continue;
-                }
+                // certified below, for all such instances at once, in parallel;
+                // an instance certified there retires (its restart, if any, is moot)
+                certify.push_back({b, src});
                 S.next_host_check = S.iterations + std::max<int64_t>(1000, 10 * o_.check_every);
             }
             if (S.iterations >= 1000 && ca.primal > o_.tol) {
@@ -1225,6 +1280,32 @@ class Batch {
             if (o_.restart && due) {
                 restart_on.push_back(b);
                 restart_src.push_back(src);
+            }
+        }
+        if (!certify.empty()) {
+            // candidates to host memory (before any restart kernel moves them),
+            // then the outward-rounded verifier on host threads
+            const size_t nc = certify.size();
+            std::vector<std::vector<double>> ox(nc), oy(nc);
+            std::vector<Accuracy> acc(nc);
+            for (size_t k = 0; k < nc; ++k) {
+                Slot &S = slots_[size_t(certify[k].first)];
+                host_point(S, point_x(S, certify[k].second), point_y(S, certify[k].second), ox[k],
+                           oy[k]);
+            }
+            batch_detail::parallel_for(nc, [&](size_t k) {
+                const Slot &S = slots_[size_t(certify[k].first)];
+                acc[k] = S.item->verifier->evaluate(ox[k], oy[k], true);
+            });
+            for (size_t k = 0; k < nc; ++k) {
+                Slot &S = slots_[size_t(certify[k].first)];
+                S.host_checks++;
+                if (acc[k].kkt <= o_.tol) {
+                    S.item->report.x = std::move(ox[k]);
+                    S.item->report.y = std::move(oy[k]);
+                    S.item->report.accuracy = acc[k];
+                    retire(S, NK_SOLVE_OPTIMAL);
+                }
             }
         }
         phase_[3] += since(t2h);
@@ -1301,9 +1382,7 @@ class Batch {
         cuda_check(cudaStreamSynchronize(stream_), "interval");
         phase_[4] += since(t3);
         auto t4 = SteadyClock::now();
-        for (int b : order_)
-            if (slots_[size_t(b)].finished)
-                close(slots_[size_t(b)]);
+        close_finished();
         phase_[5] += since(t4);
     }
 };

@@ -24,6 +24,8 @@
 #include <mutex>
 #include <numeric>
 #include <set>
+#include <atomic>
+#include <thread>
 #include <vector>
 
 #ifndef NK_SPLIT
@@ -1858,11 +1860,11 @@ nk_status nk_batch_progress(nk_batch *h, int64_t id, double progress[8]) {
         h->b.progress(id, progress);
     });
 }
-nk_status nk_batch_phase_seconds(nk_batch *h, double seconds[6]) {
+nk_status nk_batch_phase_seconds(nk_batch *h, double seconds[7]) {
     return guard([&] {
         if (!h || !seconds)
             throw nk::Error(NK_ERR_INVALID, "null argument");
-        std::memcpy(seconds, h->b.phase_seconds(), 6 * sizeof(double));
+        std::memcpy(seconds, h->b.phase_seconds(), 7 * sizeof(double));
     });
 }
 nk_status nk_batch_kernel_times(nk_batch *h, double *primal_ms, double *dual_ms) {

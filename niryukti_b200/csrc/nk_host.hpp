@@ -53,6 +53,10 @@ struct Accuracy { // vantage::Accuracy (include/vantage/vantage.hpp:78-82)
     bool finite = false;
 };
 
+// When set (per thread), host products run serially: callers that already run
+// one verifier per thread keep OpenMP from nesting teams inside them.
+void host_serial(bool serial);
+
 Csr build_csr(int64_t rows, int64_t cols, std::vector<Entry> e);
 Csr transpose(const Csr &a);
 Prepared prepare(const HostModel &src, const PrepareOptions &o);

@@ -401,9 +401,11 @@ namespace {
 long double down(long double v) { return std::nextafter(v, -std::numeric_limits<long double>::infinity()); }
 long double up(long double v) { return std::nextafter(v, std::numeric_limits<long double>::infinity()); }
 bool has_q(const HostModel &m) { return !m.Q.value.empty(); }
+thread_local bool g_host_serial = false;
+
 std::vector<double> multiply(const Csr &a, const std::vector<double> &x) {
     std::vector<double> y(size_t(a.rows));
-#pragma omp parallel for if (a.rows > 10000)
+#pragma omp parallel for if (a.rows > 10000 && !g_host_serial)
     for (int64_t i = 0; i < a.rows; i++) {
         double v = 0;
         for (auto k = a.ptr[size_t(i)]; k < a.ptr[size_t(i + 1)]; k++)
@@ -491,6 +493,8 @@ double lp_lower_bound(const HostModel &m, const Csr &at, const std::vector<doubl
     return std::nextafter(result, -INF);
 }
 } // namespace
+
+void host_serial(bool serial) { g_host_serial = serial; }
 
 bool HostModel::is_qp() const {
     return !Q.value.empty() || std::any_of(q.begin(), q.end(), [](double v) { return v != 0; });
