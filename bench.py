@@ -298,6 +298,21 @@ def solve_section(args):
             "restarts", "preprocess_seconds", "transfer_seconds", "iteration_seconds",
             "verification_seconds", "device_checks", "host_checks", "time_to_kkt")}}
         res[name]["gpu"]["budget_s"] = budget
+        # FP32 matrices first, then the closing FP64 refinement from the best
+        # reduced-precision point; accuracy of both against the FP64 solve
+        precs = ("mixed", "fp32") if "config2" not in name else ("mixed",)
+        for prec in precs if not args.no_forms else ():
+            q = solver.solve(model, tol=1e-6, time_limit=budget, iteration_limit=10**9,
+                             matrix_precision=prec, refine=True)
+            f64 = r["objective"]
+            rel = (lambda v: abs(v - f64) / (1.0 + abs(f64)))
+            res[name][f"gpu_{prec}"] = {k: q[k] for k in (
+                "status", "seconds", "iterations", "phase_iterations", "refine_iterations",
+                "phase_seconds", "kkt", "primal", "dual", "gap", "objective", "phase_kkt",
+                "phase_objective", "time_to_kkt")}
+            res[name][f"gpu_{prec}"].update(
+                budget_s=budget, objective_rel_diff_vs_fp64=rel(q["objective"]),
+                phase_objective_rel_diff_vs_fp64=rel(q["phase_objective"]))
     if not args.no_cpu:
         cmd = [sys.executable, str(pathlib.Path(__file__).resolve()), "--solve-child",
                "--cpu-threads", str(args.cpu_threads), "--cpu-solve-seconds",
@@ -525,6 +540,73 @@ def synth_pool(args):
 
 
 # ---------------------------------------------------------------- engine arm
+S_V = {"fp64": 8, "mixed": 4, "fp32": 4}
+
+
+def time_form(model, precision, steps, warmup, profile_trials):
+    """Iteration rate of one precision form of the engine on `model`: CUDA
+    events on the engine's stream around `steps` check intervals of 100 trials
+    after `warmup` untimed ones, then per-kernel event timings.  SpMV bytes
+    count matrix values at the form's width (8 B FP64, 4 B FP32)."""
+    import torch
+    from niryukti_b200 import engine
+    m, n, nnz = model.m, model.n, model.nnz
+    tau, sigma = step_sizes(model)
+    g = engine.PdhgBackend(model, adaptive=True, graphs=True, precision=precision)
+    try:
+        ext = torch.cuda.ExternalStream(g.stream())
+        for _ in range(warmup):
+            g.advance(TRIALS_PER_STEP, tau, sigma)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        for _ in range(steps):
+            g.advance(TRIALS_PER_STEP, tau, sigma)
+        e1.record(ext)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        it_s = steps * TRIALS_PER_STEP / (ms / 1e3)
+        s_v = S_V[precision]
+        ms_p, ms_d = g.profile(profile_trials, tau, sigma)
+        bp, bd = fused_kernel_bytes(m, n, nnz, s_v)
+        return {"matrix_precision": precision, "iterations_per_s": it_s,
+                "ms_per_iteration": 1e3 / it_s,
+                "spmv_GBps": it_s * iteration_spmv_bytes(m, n, nnz, s_v) / 1e9,
+                "whole_iteration_GBps": it_s * (bp + bd) / 1e9,
+                "kernels": {"primal_kernel": {"ms": ms_p, "bytes": bp, "GBps": bp / ms_p / 1e6},
+                            "dual_kernel": {"ms": ms_d, "bytes": bd, "GBps": bd / ms_d / 1e6}},
+                "schedule": g.schedule_info()}
+    finally:
+        del g
+        torch.cuda.synchronize()
+
+
+def config3_section(args):
+    """Config 3: the block-angular planning LP (64 blocks of 20,000 x 40,000
+    with 6 nonzeros per column, 2,000 linking rows over 5% of all columns
+    each), iteration rate in FP64 and with FP32 matrices."""
+    import torch
+    from niryukti_b200 import synth
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    model = synth.block_angular_lp(blocks=args.config3_blocks)
+    gen_s = time.perf_counter() - t0
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    out = {"workload": f"config3_block_angular_b{args.config3_blocks}_20000x40000_link2000",
+           "m": model.m, "n": model.n, "nnz": model.nnz, "generate_s": gen_s,
+           "peak_GBps": peak, "forms": {}}
+    for prec in ("fp64", "mixed"):
+        r = time_form(model, prec, args.steps, args.warmup, args.profile_trials)
+        r["spmv_frac_of_measured_peak"] = r["spmv_GBps"] / peak
+        r["whole_iteration_frac"] = r["whole_iteration_GBps"] / peak
+        out["forms"][prec] = r
+    return out
+
+
 def engine_arm(args, world, rank, local):
     import torch
     from niryukti_b200 import engine
@@ -586,7 +668,7 @@ def engine_arm(args, world, rank, local):
         # DRAM bytes per launch from the ncu capture of the config-2 shape at half
         # size (profiles/fused_pdhg_kernels_config2_scaled_half.md: read + write),
         # scaled by 2: every unit (nonzeros, rows, columns) doubles
-        traffic = {"primal_kernel": 2 * 183.26e6, "dual_kernel": 2 * 166.60e6}[top]
+        traffic = {"primal_kernel": 2 * 181.32e6, "dual_kernel": 2 * 166.24e6}[top]
         traffic_source = "ncu dram__bytes_read.sum + dram__bytes_write.sum at scale 0.5, x2"
     roofline = {"bound": "hbm", "kernel": top, "achieved": kernels[top]["GBps"], "peak": peak,
                 "unit": "GB/s", "frac": kernels[top]["GBps"] / peak, "traffic": traffic,
@@ -600,9 +682,9 @@ def engine_arm(args, world, rank, local):
     outs = [torch.empty(k, dtype=torch.float64).pin_memory() for k in (n, m, n, m)]
     hxn, hyn = hx.numpy(), hy.numpy()
     on = [o.numpy() for o in outs]
-    cx, cy, cxa, cya = g.candidates()
-    hxn[:] = cx
-    hyn[:] = cy
+    g.candidates(out=on)
+    hxn[:] = on[0]
+    hyn[:] = on[1]
     barrier()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(ext)
@@ -610,9 +692,7 @@ def engine_arm(args, world, rank, local):
     for _ in range(args.e2e_steps):
         g.reset(hxn, hyn)
         g.advance(TRIALS_PER_STEP, tau, sigma)
-        res = g.candidates()
-        for dst, src in zip(on, res):
-            dst[:] = src
+        g.candidates(out=on)  # straight into the pinned host buffers
     f1.record(ext)
     f1.synchronize()
     wall = time.perf_counter() - w0
@@ -623,6 +703,15 @@ def engine_arm(args, world, rank, local):
         e2e_ms = float(t.item())
     e2e_value = world * (args.e2e_steps * TRIALS_PER_STEP / (e2e_ms / 1e3)) * \
         iteration_spmv_bytes(m, n, nnz, s_v) / 1e9
+
+    del g
+    forms = {}
+    if not args.no_forms:
+        # the same LP with FP32 matrices: MIXED (FP64 gathers and sums) and FP32
+        # (FP32 gathers and sums); iterates, averages and reductions stay FP64
+        for prec in ("mixed", "fp32"):
+            if prec != args.precision:
+                forms[prec] = time_form(model, prec, args.steps, args.warmup, args.profile_trials)
 
     if rank != 0:
         if dist:
@@ -656,8 +745,8 @@ def engine_arm(args, world, rank, local):
                     "h2d_bytes_per_step": 8 * (n + m), "d2h_bytes_per_step": 16 * (n + m),
                     "path": "nk_pdhg_reset + nk_pdhg_advance(100) + nk_pdhg_candidates"},
             "gpu_launches": 2 * (args.steps * TRIALS_PER_STEP),
-            "clocks": clocks.summary(), "accepted_trials": accepted}
-    del g
+            "clocks": clocks.summary(), "accepted_trials": accepted,
+            "precision_forms": forms}
     if not args.no_solve:
         line["solve"] = solve_section(args)
     if not args.no_batch:
@@ -710,6 +799,11 @@ def main():
     ap.add_argument("--batch-precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--batch-cpu-sample", type=int, default=4,
                     help="smallest sampled instances also solved by the reference on the CPU")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the FP32-matrix forms of the config-2 iteration rate")
+    ap.add_argument("--config3", action="store_true",
+                    help="print only the config-3 block-angular iteration-rate section")
+    ap.add_argument("--config3-blocks", type=int, default=64)
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per launch of the top kernel from an ncu capture")
     args = ap.parse_args()
@@ -725,6 +819,9 @@ def main():
         return
     if args.serve:
         print(json.dumps({"serve": serve_section(args)}))
+        return
+    if args.config3:
+        print(json.dumps({"config3": config3_section(args)}))
         return
     world, rank, local = dist_setup()
     if args.impl == "reference":

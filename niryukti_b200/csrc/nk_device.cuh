@@ -24,11 +24,19 @@
 #ifndef NK_MIN_BLOCKS
 #define NK_MIN_BLOCKS 4 // CTAs per SM the fused kernels are register-bounded for
 #endif
+#ifndef NK_SPLIT_PIPE
+#define NK_SPLIT_PIPE 0 // 1: software-pipelined dot for split-row segments
+#endif
+#ifndef NK_DUAL_GATHER
+#define NK_DUAL_GATHER 0 // gather flavour of the dual kernel's dx loads (gather_as)
+#endif
 #ifndef NK_PREFETCH
 #define NK_PREFETCH 1 // 1: load a row's epilogue vectors before its dot product
 #endif
 
 namespace nk {
+
+constexpr int kDualGather = NK_DUAL_GATHER;
 
 // Device-resident control state.  The first eleven fields keep the meaning of
 // the reference's `state` vector (src/cuda.cu:224-225,601).
@@ -145,11 +153,15 @@ __device__ __forceinline__ bool split_chunk(double *wpart /* this warp's 32 */, 
 // chunk combine.  Kept out of line so that the register budget of the kernels'
 // main path does not carry it.  init_vec (may be null) gives the row sum's
 // start; on true, *row and *total hold the completed row.
-template <class Acc, class V, class I, class X>
+template <class Acc, int G = 0, class V, class I, class X>
 __device__ __noinline__ bool split_lane(const Sell<V, I> M, int64_t vr, int len,
                                         const X *__restrict__ x, const double *init_vec,
                                         double *wpart, int64_t *row, double *total) {
-    const double part = double(sell_dot<Acc, kUnrollSplit>(M, vr, len, Acc(0), x));
+#if NK_SPLIT_PIPE
+    const double part = double(sell_dot_pipelined<Acc, kUnrollSplit>(M, vr, len, Acc(0), x));
+#else
+    const double part = double(sell_dot<Acc, kUnrollSplit, G>(M, vr, len, Acc(0), x));
+#endif
     const int4 sg = M.seg[vr];
     *row = sg.x;
     const double init = (sg.x >= 0 && init_vec) ? init_vec[sg.x] : 0.;
@@ -204,7 +216,8 @@ __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS)
             bad |= !isfinite(t);
         };
         const int lane = threadIdx.x & 31;
-        for (int64_t ch = first_chunk(); ch * 32 < At.nv; ch += chunk_stride()) {
+        WarpChunks<V, I> chunks(At);
+        for (int64_t ch; chunks.next(&ch);) {
             const int64_t vr = ch * 32 + lane;
             if (vr >= At.nv)
                 continue;
@@ -334,7 +347,8 @@ __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS) dual_kernel(Sell<V, I
             bad |= !isfinite(bar) || !isfinite(t) || !isfinite(delta);
         };
         const int lane = threadIdx.x & 31;
-        for (int64_t ch = first_chunk(); ch * 32 < A.nv; ch += chunk_stride()) {
+        WarpChunks<V, I> chunks(A);
+        for (int64_t ch; chunks.next(&ch);) {
             const int64_t vr = ch * 32 + lane;
             if (vr >= A.nv)
                 continue;
@@ -347,9 +361,9 @@ __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS) dual_kernel(Sell<V, I
 #endif
                 double delta;
                 if constexpr (FP32G)
-                    delta = double(sell_dot<Acc>(A, vr, len, Acc(0), v.dx32));
+                    delta = double(sell_dot<Acc, kUnroll, kDualGather>(A, vr, len, Acc(0), v.dx32));
                 else
-                    delta = double(sell_dot<Acc>(A, vr, len, Acc(0), v.dx));
+                    delta = double(sell_dot<Acc, kUnroll, kDualGather>(A, vr, len, Acc(0), v.dx));
 #if NK_PREFETCH
                 finish(i, delta, yi, axi, rli, rui, ai);
 #else
@@ -360,9 +374,9 @@ __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS) dual_kernel(Sell<V, I
                 double delta;
                 bool done;
                 if constexpr (FP32G)
-                    done = split_lane<Acc>(A, vr, len, v.dx32, nullptr, wpart[threadIdx.x >> 5], &i, &delta);
+                    done = split_lane<Acc, kDualGather>(A, vr, len, v.dx32, nullptr, wpart[threadIdx.x >> 5], &i, &delta);
                 else
-                    done = split_lane<Acc>(A, vr, len, v.dx, nullptr, wpart[threadIdx.x >> 5], &i, &delta);
+                    done = split_lane<Acc, kDualGather>(A, vr, len, v.dx, nullptr, wpart[threadIdx.x >> 5], &i, &delta);
                 if (done)
                     finish(i, delta, y[i], ax[i], v.rl[i], v.ru[i], pending ? v.ya[i] : 0.);
             }

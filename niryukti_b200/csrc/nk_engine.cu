@@ -23,13 +23,18 @@
 #include <memory>
 #include <mutex>
 #include <numeric>
+#include <queue>
+#include <utility>
 #include <set>
 #include <atomic>
 #include <thread>
 #include <vector>
 
+#ifndef NK_BALANCED
+#define NK_BALANCED 1 // 1: fused kernels follow the balanced warp schedule, 0: round-robin
+#endif
 #ifndef NK_SPLIT
-#define NK_SPLIT 64 // rows with more entries are split into virtual rows of this length
+#define NK_SPLIT 128 // rows with more entries are split into virtual rows of this length
 #endif
 #ifndef NK_SPLIT_MAX
 #define NK_SPLIT_MAX 256 // longest segment of a row that spans several chunks
@@ -61,6 +66,19 @@ struct SellMatrix {
     DevBuf<int4> seg;
     DevBuf<double> slots;
     DevBuf<unsigned> counters;
+    std::vector<int32_t> chunk_len; // host: padded length of each chunk
+    DevBuf<int64_t> woff, wlist;    // balanced warp schedule of the fused kernels
+
+    // The view the fused trial kernels use: with the balanced warp schedule
+    // (built for their persistent grid).
+    template <class V, class I> Sell<V, I> fused_view() const {
+        Sell<V, I> s = view<V, I>();
+#if NK_BALANCED
+        s.woff = woff.p;
+        s.wlist = wlist.p;
+#endif
+        return s;
+    }
 
     template <class V, class I> Sell<V, I> view() const {
         Sell<V, I> s;
@@ -84,7 +102,8 @@ struct SellMatrix {
     }
     size_t device_bytes() const {
         return cptr.bytes() + len.bytes() + idx32.bytes() + idx64.bytes() + val64.bytes() +
-               val32.bytes() + seg.bytes() + slots.bytes() + counters.bytes();
+               val32.bytes() + seg.bytes() + slots.bytes() + counters.bytes() + woff.bytes() +
+               wlist.bytes();
     }
 };
 
@@ -219,6 +238,9 @@ void build_sell(SellMatrix &M, int64_t rows, int64_t cols, const std::vector<int
     M.nsv = P.nsv;
     M.nsr = P.nsr;
     M.padded = P.cptr.back();
+    M.chunk_len.resize(P.cptr.size() - 1);
+    for (size_t c = 0; c + 1 < P.cptr.size(); ++c)
+        M.chunk_len[c] = int32_t((P.cptr[c + 1] - P.cptr[c]) / 32);
     upload_vector(M.cptr, P.cptr, s);
     upload_vector(M.len, P.len, s);
     upload_vector(M.seg, P.seg, s);
@@ -456,8 +478,8 @@ struct Engine {
     template <class Acc, class V, class I> void launch_trial_t() {
         Vecs v = vecs();
         constexpr bool F32 = sizeof(Acc) == 4;
-        auto at = At.view<V, I>();
-        auto a = A.view<V, I>();
+        auto at = At.fused_view<V, I>();
+        auto a = A.fused_view<V, I>();
         auto qm = Q.view<V, I>();
         if (ev[0])
             cudaEventRecord(ev[0], stream);
@@ -643,23 +665,28 @@ struct Engine {
                        "upload");
     }
     // Vector transfers in the caller's order (columns: col_perm, rows: row_perm).
+    // With sync = false the transfer is only enqueued: the caller synchronises
+    // the stream before it reads (download) or reuses (upload) the host buffer.
+    // Transfers through the same scratch stay ordered by the stream.
     void download_perm(double *host, const double *dev, int64_t len, const DevBuf<int64_t> &perm,
-                       DevBuf<double> &scratch) {
+                       DevBuf<double> &scratch, bool sync = true) {
         if (!len || !host)
             return;
         scatter_vec<<<grid_for(len), kThreads, 0, stream>>>(len, perm.p, dev, scratch.p);
         cuda_check(cudaGetLastError(), "scatter");
         download(host, scratch.p, len);
-        cuda_check(cudaStreamSynchronize(stream), "download");
+        if (sync)
+            cuda_check(cudaStreamSynchronize(stream), "download");
     }
     void upload_perm(double *dev, const double *host, int64_t len, const DevBuf<int64_t> &perm,
-                     DevBuf<double> &scratch) {
+                     DevBuf<double> &scratch, bool sync = true) {
         if (!len)
             return;
         upload(scratch.p, host, len);
         gather_vec<<<grid_for(len), kThreads, 0, stream>>>(len, perm.p, scratch.p, dev);
         cuda_check(cudaGetLastError(), "gather");
-        cuda_check(cudaStreamSynchronize(stream), "upload");
+        if (sync)
+            cuda_check(cudaStreamSynchronize(stream), "upload");
     }
     void download_x(double *h, const double *d) { download_perm(h, d, n, col_perm, scratch_n); }
     void download_y(double *h, const double *d) { download_perm(h, d, m, row_perm, scratch_m); }
@@ -670,10 +697,11 @@ struct Engine {
         flush();
         sync_ctl();
         int cur = host_ctl->cur;
-        download_x(hx, x[cur].p);
-        download_y(hy, y[cur].p);
-        download_x(hxa, xa.p);
-        download_y(hya, ya.p);
+        // four stream-ordered transfers, one synchronisation
+        download_perm(hx, x[cur].p, n, col_perm, scratch_n, false);
+        download_perm(hy, y[cur].p, m, row_perm, scratch_m, false);
+        download_perm(hxa, xa.p, n, col_perm, scratch_n, false);
+        download_perm(hya, ya.p, m, row_perm, scratch_m, false);
         refresh_activity(cur); // rebase A*x like the reference (src/cuda.cu:874-891)
         cuda_check(cudaStreamSynchronize(stream), "candidates");
     }
@@ -735,11 +763,12 @@ struct Engine {
     void reset(const double *hx, const double *hy) {
         sync_ctl();
         int cur = host_ctl->cur;
-        upload_x(x[cur].p, hx);
-        upload_y(y[cur].p, hy);
+        upload_perm(x[cur].p, hx, n, col_perm, scratch_n, false);
+        upload_perm(y[cur].p, hy, m, row_perm, scratch_m, false);
         refresh_y32(cur);
         refresh_activity(cur);
         restart_state(cur);
+        cuda_check(cudaStreamSynchronize(stream), "reset"); // the caller may reuse hx, hy
     }
 
     double monitor() {
@@ -958,6 +987,104 @@ struct Engine {
         return b;
     }
 };
+
+// Balanced warp schedule for a persistent grid of `warps` warps (kWarps per
+// CTA, all CTAs resident at once: occupancy_grid never launches more).
+//
+// Two costs per chunk of padded length L:
+//  * memory work, what an SM's load/store path spends on it: one scattered
+//    sector per gathered entry, the entries' index and value stream, and the
+//    row epilogue's vector traffic (about 44 L + 70 sectors);
+//  * a warp's chain of dependent round trips: per round of kUnroll entries an
+//    index/value load and then the gathers it feeds, one round per leftover
+//    entry, plus the epilogue (and the segment combine of split rows).
+// Level 1 spreads the chunks over the CTAs by memory work, level 2 over the
+// warps of each CTA by chain length; both are longest-first list scheduling
+// (the next chunk goes to the least-loaded CTA or warp, ties to the lowest
+// index).  Every SM holds the same number of CTAs, so balanced CTAs mean
+// balanced SMs whatever the block scheduler's placement.  Rows are sorted by
+// length, so plain round-robin puts the long split-row chunks on the lowest
+// warps, hence on a subset of the SMs, which then set the kernel's time.
+// Which warp runs a chunk changes no row sum, and the per-CTA partial sums are
+// fixed for a given schedule, so results stay deterministic.
+void build_schedule(SellMatrix &M, int64_t warps, cudaStream_t s) {
+    const int64_t nch = int64_t(M.chunk_len.size());
+    const int64_t ctas = std::max<int64_t>(1, warps / kWarps);
+    warps = ctas * kWarps;
+    const int64_t split_chunks = M.nsv / 32;
+    std::vector<int64_t> work(static_cast<size_t>(nch)), chain(static_cast<size_t>(nch));
+    for (int64_t c = 0; c < nch; ++c) {
+        const int64_t L = M.chunk_len[size_t(c)];
+        const bool split = c < split_chunks;
+        const int64_t u = split ? kUnrollSplit : kUnroll;
+        work[size_t(c)] = 44 * L + (split ? 100 : 70);
+        chain[size_t(c)] = (split && NK_SPLIT_PIPE ? (L + u - 1) / u + 1 : 2 * (L / u) + 2 * (L % u)) +
+                           (split ? 6 : 4);
+    }
+    using Slot = std::pair<int64_t, int64_t>; // (load so far, machine)
+    auto lpt = [](const std::vector<int64_t> &items, const std::vector<int64_t> &cost,
+                  int64_t machines, std::vector<int64_t> &owner) {
+        std::vector<int64_t> order(items);
+        std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
+            return cost[size_t(a)] > cost[size_t(b)];
+        });
+        std::priority_queue<Slot, std::vector<Slot>, std::greater<Slot>> heap;
+        for (int64_t k = 0; k < machines; ++k)
+            heap.push({0, k});
+        for (int64_t c : order) {
+            Slot t = heap.top();
+            heap.pop();
+            owner[size_t(c)] = t.second;
+            heap.push({t.first + cost[size_t(c)], t.second});
+        }
+        return order; // assignment order, costliest first
+    };
+    std::vector<int64_t> all(static_cast<size_t>(nch)), cta(static_cast<size_t>(nch));
+    for (int64_t c = 0; c < nch; ++c)
+        all[size_t(c)] = c;
+    lpt(all, work, ctas, cta);
+    // chunks of each CTA, then its warps
+    std::vector<int64_t> cstart(static_cast<size_t>(ctas + 1), 0);
+    for (int64_t c = 0; c < nch; ++c)
+        ++cstart[size_t(cta[size_t(c)] + 1)];
+    for (int64_t b = 0; b < ctas; ++b)
+        cstart[size_t(b + 1)] += cstart[size_t(b)];
+    std::vector<int64_t> bychunk(static_cast<size_t>(std::max<int64_t>(1, nch)));
+    {
+        std::vector<int64_t> pos(cstart.begin(), cstart.end() - 1);
+        for (int64_t c = 0; c < nch; ++c)
+            bychunk[size_t(pos[size_t(cta[size_t(c)])]++)] = c;
+    }
+    std::vector<int64_t> off(static_cast<size_t>(warps + 1), 0), seq;
+    seq.reserve(size_t(nch));
+    std::vector<int64_t> local_owner(static_cast<size_t>(nch));
+    std::vector<std::vector<int64_t>> lists(static_cast<size_t>(kWarps));
+    for (int64_t b = 0; b < ctas; ++b) {
+        std::vector<int64_t> mine(bychunk.begin() + cstart[size_t(b)],
+                                  bychunk.begin() + cstart[size_t(b + 1)]);
+        for (auto &l : lists)
+            l.clear();
+        for (int64_t c : lpt(mine, chain, kWarps, local_owner))
+            lists[size_t(local_owner[size_t(c)])].push_back(c);
+        for (int k = 0; k < kWarps; ++k) {
+            off[size_t(b * kWarps + k + 1)] = int64_t(lists[size_t(k)].size());
+            seq.insert(seq.end(), lists[size_t(k)].begin(), lists[size_t(k)].end());
+        }
+    }
+    for (int64_t w = 0; w < warps; ++w)
+        off[size_t(w + 1)] += off[size_t(w)];
+    // every chunk exactly once
+    std::vector<char> seen(static_cast<size_t>(nch), 0);
+    for (int64_t c : seq)
+        if (c < 0 || c >= nch || seen[size_t(c)]++)
+            throw Error(NK_ERR_INVALID, "internal: warp schedule is not a permutation");
+    if (int64_t(seq.size()) != nch || off[size_t(warps)] != nch)
+        throw Error(NK_ERR_INVALID, "internal: warp schedule size");
+    if (seq.empty())
+        seq.push_back(0);
+    upload_vector(M.woff, off, s);
+    upload_vector(M.wlist, seq, s);
+}
 
 // Persistent grid: as many CTAs as fit on the device at once, at most one warp
 // per SELL chunk.
@@ -1186,6 +1313,8 @@ Engine *create_engine(const nk_csr *Ah, const nk_csr *Qh, const double *hc, cons
         E->wide ? configure<double, float, int64_t>(*E) : configure<double, float, int32_t>(*E);
     else
         E->wide ? configure<float, float, int64_t>(*E) : configure<float, float, int32_t>(*E);
+    build_schedule(E->At, int64_t(E->grid_p) * kWarps, s);
+    build_schedule(E->A, int64_t(E->grid_d) * kWarps, s);
     E->part_p.alloc(size_t(E->grid_p));
     E->part_d.alloc(size_t(2 * E->grid_d));
     E->ctl.alloc(1);

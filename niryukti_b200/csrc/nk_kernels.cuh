@@ -23,6 +23,25 @@ template <class T> __device__ __forceinline__ T stream_load(const T *p) {
 }
 template <class T> __device__ __forceinline__ T gather_load(const T *p) { return __ldg(p); }
 
+// Gather flavours: 0 read-only path (L1-allocating), 1 read-only without L1
+// allocation (a gathered line is rarely reused from L1 when the vector is much
+// larger than L1), 2 L2 only.
+template <int G, class T> __device__ __forceinline__ T gather_as(const T *p) {
+    if constexpr (G == 1 && sizeof(T) == 8) {
+        double v;
+        asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+        return T(v);
+    } else if constexpr (G == 1 && sizeof(T) == 4) {
+        float v;
+        asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+        return T(v);
+    } else if constexpr (G == 2) {
+        return __ldcg(p);
+    } else {
+        return __ldg(p);
+    }
+}
+
 // Deterministic CTA reduction of NV doubles (fixed tree); result in thread 0.
 template <int NV> __device__ __forceinline__ void cta_sum(double (&v)[NV], double *smem /* kWarps*NV */) {
 #pragma unroll

@@ -45,12 +45,43 @@ template <class V, class I> struct Sell {
                            //   segments, counter (-1: the row lies in one chunk)}
     double *slots;         // per split segment: partial sum
     unsigned *counters;    // per split row: arrivals (reset by the last one)
+    // Balanced warp schedule of the fused kernels (null: round-robin): the
+    // chunks of persistent warp w are wlist[woff[w] .. woff[w+1]).
+    const int64_t *woff = nullptr;
+    const int64_t *wlist = nullptr;
+};
+
+// Iterates the SELL chunks of the calling warp: the balanced schedule when the
+// matrix carries one (the grid it was built for), else round-robin over the
+// persistent grid.  Every lane of a warp sees the same chunks.
+template <class V, class I> struct WarpChunks {
+    const Sell<V, I> &M;
+    int64_t k, end, stride;
+    __device__ __forceinline__ explicit WarpChunks(const Sell<V, I> &m) : M(m) {
+        const int64_t w = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+        if (M.woff) {
+            k = M.woff[w];
+            end = M.woff[w + 1];
+            stride = 1;
+        } else {
+            k = w;
+            end = (M.nv + 31) >> 5;
+            stride = (int64_t(gridDim.x) * blockDim.x) >> 5;
+        }
+    }
+    __device__ __forceinline__ bool next(int64_t *ch) {
+        if (k >= end)
+            return false;
+        *ch = M.woff ? M.wlist[k] : k;
+        k += stride;
+        return true;
+    }
 };
 
 // Sequential dot product of virtual row v (entries in CSR order) starting
 // from acc; U entries' loads are issued before their products are added.
 // Used inside the fused PDHG kernels, where registers are scarce.
-template <class Acc, int U = kUnroll, class V, class I, class X>
+template <class Acc, int U = kUnroll, int G = 0, class V, class I, class X>
 __device__ __forceinline__ Acc sell_dot(const Sell<V, I> &M, int64_t v, int len, Acc acc,
                                         const X *__restrict__ x) {
     const int64_t base = M.cptr[v >> 5] + (v & 31);
@@ -68,14 +99,14 @@ __device__ __forceinline__ Acc sell_dot(const Sell<V, I> &M, int64_t v, int len,
         X g[U];
 #pragma unroll
         for (int u = 0; u < U; ++u)
-            g[u] = gather_load(x + j[u]);
+            g[u] = gather_as<G>(x + j[u]);
 #pragma unroll
         for (int u = 0; u < U; ++u)
             acc = acc + Acc(w[u]) * Acc(g[u]);
     }
     for (; k < len; ++k)
         acc = acc + Acc(stream_load(vp + int64_t(k) * 32)) *
-                        Acc(gather_load(x + stream_load(ip + int64_t(k) * 32)));
+                        Acc(gather_as<G>(x + stream_load(ip + int64_t(k) * 32)));
     return acc;
 }
 

@@ -190,9 +190,18 @@ class PdhgBackend:
         check(self._L.nk_pdhg_monitor(self._h, C.byref(v)))
         return v.value
 
-    def candidates(self):
-        x, y = np.empty(self.n), np.empty(self.m)
-        xa, ya = np.empty(self.n), np.empty(self.m)
+    def candidates(self, out=None):
+        """(x, y, x_avg, y_avg) in the caller's order; rebases A x.  ``out``
+        (optional): four preallocated C-contiguous float64 arrays of n, m, n
+        and m entries to fill, e.g. views of pinned host memory."""
+        if out is None:
+            out = (np.empty(self.n), np.empty(self.m), np.empty(self.n), np.empty(self.m))
+        else:
+            for a, k in zip(out, (self.n, self.m, self.n, self.m)):
+                if a.dtype != np.float64 or a.shape != (k,) or not a.flags.c_contiguous:
+                    raise ValueError("candidates(out=...) needs C-contiguous float64 arrays "
+                                     "of n, m, n and m entries")
+        x, y, xa, ya = out
         check(self._L.nk_pdhg_candidates(self._h, _d(x), _d(y), _d(xa), _d(ya)))
         return x, y, xa, ya
 

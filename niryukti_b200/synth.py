@@ -271,19 +271,28 @@ def block_angular_lp(blocks: int = 64, block_rows: int = 20_000, block_cols: int
     local = rng.integers(0, block_rows, size=cols_b.size)
     local = _dedupe_pairs(rng, cols_b, local, block_rows)
     rows_b = blk * block_rows + local
-    # linking part
+    vals_b = rng.uniform(0.1, 2.0, rows_b.size)
+    vals_b[rng.random(rows_b.size) < 0.3] *= -1
+    ptr_b, idx_b, val_b = _canonical_csr(rows_b, cols_b, vals_b, mb)
+    del rows_b, cols_b, vals_b, blk, local
+    # linking part: rows after the block rows, each already in column order, so
+    # the CSR is the block CSR with the linking rows appended (no global sort)
     per_link = int(round(linking_frac * n))
-    rows_l = np.repeat(np.arange(mb, m, dtype=np.int64), per_link)
-    cols_l = np.empty(rows_l.size, dtype=np.int64)
+    nb = idx_b.size
+    idx = np.empty(nb + linking_rows * per_link, dtype=np.int64)
+    idx[:nb] = idx_b
     for r in range(linking_rows):
-        cols_l[r * per_link:(r + 1) * per_link] = np.sort(rng.choice(n, per_link, replace=False))
-    rows = np.concatenate([rows_b, rows_l])
-    cols = np.concatenate([cols_b, cols_l])
-    del rows_b, rows_l, cols_b, cols_l, blk, local
-    vals = rng.uniform(0.1, 2.0, rows.size)
-    vals[rng.random(rows.size) < 0.3] *= -1
-    ptr, idx, val = _canonical_csr(rows, cols, vals, m)
-    del rows, cols, vals
+        idx[nb + r * per_link:nb + (r + 1) * per_link] = np.sort(
+            rng.choice(n, per_link, replace=False))
+    val = np.empty(idx.size, dtype=np.float64)
+    val[:nb] = val_b
+    vl = rng.uniform(0.1, 2.0, idx.size - nb)
+    vl[rng.random(vl.size) < 0.3] *= -1
+    val[nb:] = vl
+    ptr = np.empty(m + 1, dtype=np.int64)
+    ptr[:mb + 1] = ptr_b
+    ptr[mb + 1:] = nb + per_link * np.arange(1, linking_rows + 1, dtype=np.int64)
+    del idx_b, val_b, vl
     x0 = rng.uniform(0, x_hi, n)
     ax0 = csr_matvec(ptr, idx, val, x0, m)
     rl = ax0.copy()

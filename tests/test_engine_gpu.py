@@ -191,6 +191,12 @@ def test_sparse_qp_parity(gpu, oracle):
 
 @pytest.mark.parametrize("seed", [1, 2])
 def test_random_lp_adaptive_parity(gpu, oracle, seed):
+    """Adaptive steps on a power-law LP with rows of up to 6,000 entries and row
+    scales over four decades.  Tolerance 1e-8 relative after 40 accepted steps:
+    the device adds a long row's segments and the step rule's sums in a fixed
+    tree, the CPU loop adds them one by one, and the adaptive step factor (a
+    ratio of those sums) carries those last-bit differences from one step to
+    the next."""
     m = synth.power_law_lp(m=4000, n=8000, nnz=80000, seed=seed, len_hi=6000)
     cpu = oracle.model(m).backend(np.zeros(m.n), np.zeros(m.m), adaptive=True)
     g = gpu.PdhgBackend(m, adaptive=True, graphs=True)
@@ -199,7 +205,7 @@ def test_random_lp_adaptive_parity(gpu, oracle, seed):
         done = advance_to(g, done + cpu.advance(10, 0.01, 0.01), 0.01, 0.01, done)
         assert g.rejected_steps() == cpu.rejected_steps()
         for u, w in zip(g.candidates(), cpu.candidates()):
-            near(u, w, 1e-9)
+            near(u, w, 1e-8)
 
 
 def test_fp32_precision_tracks_fp64(gpu):
