@@ -127,6 +127,23 @@ class Clocks:
                 "samples": len(rows)}
 
 
+def max_over_ranks(value: float, dist=None, device: str = "cuda") -> float:
+    """The slowest rank's time: every rank contributes its own CUDA-event time
+    and all of them get the maximum (no-op on one process)."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(world: int, units_per_rank: float, ms_max: float) -> float:
+    """Whole-job rate of independent replicas: the units all ranks processed
+    over the max-over-ranks time (weak scaling)."""
+    return world * units_per_rank / (ms_max / 1e3)
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -643,14 +660,10 @@ def engine_arm(args, world, rank, local):
         e1.record(ext)
         e1.synchronize()
     barrier()
-    ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), dist)
     trials = args.steps * TRIALS_PER_STEP
     it_s = trials / (ms / 1e3)
-    value = world * it_s * iteration_spmv_bytes(m, n, nnz, s_v) / 1e9
+    value = replica_rate(world, trials, ms) * iteration_spmv_bytes(m, n, nnz, s_v) / 1e9
 
     # per-kernel durations (CUDA events around each kernel, same stream)
     ms_p, ms_d = g.profile(args.profile_trials, tau, sigma)
@@ -696,12 +709,8 @@ def engine_arm(args, world, rank, local):
     f1.record(ext)
     f1.synchronize()
     wall = time.perf_counter() - w0
-    e2e_ms = max(f0.elapsed_time(f1), 1e3 * wall)
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * (args.e2e_steps * TRIALS_PER_STEP / (e2e_ms / 1e3)) * \
+    e2e_ms = max_over_ranks(max(f0.elapsed_time(f1), 1e3 * wall), dist)
+    e2e_value = replica_rate(world, args.e2e_steps * TRIALS_PER_STEP, e2e_ms) * \
         iteration_spmv_bytes(m, n, nnz, s_v) / 1e9
 
     del g
