@@ -48,11 +48,12 @@ def iteration_spmv_bytes(m, n, nnz, s_v=8):
     return spmv_bytes(m, n, nnz, s_v) + spmv_bytes(n, m, nnz, s_v)
 
 
-def fused_kernel_bytes(m, n, nnz, s_v=8):
+def fused_kernel_bytes(m, n, nnz, s_v=8, diag_q=False):
     """Algorithmic bytes of the two fused kernels of one trial.
-    primal: A^T (nnz, n+1 ptr) + gather y (m) + read x, c, q, lb, ub, xa + write trial, dx, xa (n)
+    primal: A^T (nnz, n+1 ptr) + gather y (m) + read x, c, lb, ub, xa (and q when the model has
+            a diagonal quadratic term; an LP's q is never read) + write trial, dx, xa (n)
     dual:   A (nnz, m+1 ptr) + gather dx (n) + read y, Ax, rl, ru, ya + write trial, Ax', ya (m)"""
-    primal = nnz * (s_v + 4) + (n + 1) * 4 + m * 8 + 9 * 8 * n
+    primal = nnz * (s_v + 4) + (n + 1) * 4 + m * 8 + (9 if diag_q else 8) * 8 * n
     dual = nnz * (s_v + 4) + (m + 1) * 4 + n * 8 + 8 * 8 * m
     return primal, dual
 
@@ -585,7 +586,7 @@ def time_form(model, precision, steps, warmup, profile_trials):
         it_s = steps * TRIALS_PER_STEP / (ms / 1e3)
         s_v = S_V[precision]
         ms_p, ms_d = g.profile(profile_trials, tau, sigma)
-        bp, bd = fused_kernel_bytes(m, n, nnz, s_v)
+        bp, bd = fused_kernel_bytes(m, n, nnz, s_v, diag_q=bool(np.any(model.q)))
         return {"matrix_precision": precision, "iterations_per_s": it_s,
                 "ms_per_iteration": 1e3 / it_s,
                 "spmv_GBps": it_s * iteration_spmv_bytes(m, n, nnz, s_v) / 1e9,
@@ -667,7 +668,7 @@ def engine_arm(args, world, rank, local):
 
     # per-kernel durations (CUDA events around each kernel, same stream)
     ms_p, ms_d = g.profile(args.profile_trials, tau, sigma)
-    bp, bd = fused_kernel_bytes(m, n, nnz, s_v)
+    bp, bd = fused_kernel_bytes(m, n, nnz, s_v, diag_q=bool(np.any(model.q)))
     kernels = {"primal_kernel": {"ms": ms_p, "bytes": bp, "GBps": bp / ms_p / 1e6},
                "dual_kernel": {"ms": ms_d, "bytes": bd, "GBps": bd / ms_d / 1e6}}
     top = max(kernels, key=lambda k: kernels[k]["ms"])
@@ -747,7 +748,7 @@ def engine_arm(args, world, rank, local):
                        "adaptive": True, "graphs": True, "parallelism": f"replicas{world}",
                        "l2": "inputs larger than L2 (about 730 MB per iteration)"},
             "iterations_per_s": it_s,
-            "whole_iteration_GBps": it_s * sum(fused_kernel_bytes(m, n, nnz, s_v)) / 1e9,
+            "whole_iteration_GBps": it_s * (bp + bd) / 1e9,
             "kernels": kernels, "schedule": sched, "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "GB/s",

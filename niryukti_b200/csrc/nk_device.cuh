@@ -225,7 +225,8 @@ __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS)
             if (!SPLIT || vr >= At.nsv) {
                 const int64_t j = vr - At.nsv + At.nsr;
 #if NK_PREFETCH // the epilogue's loads do not depend on the dot product: issue them first
-                const double xj = x[j], cj = v.c[j], qj = v.q[j], lj = v.lb[j], uj = v.ub[j];
+                const double xj = x[j], cj = v.c[j], qj = v.q ? v.q[j] : 0., lj = v.lb[j],
+                             uj = v.ub[j];
                 const double aj = pending ? v.xa[j] : 0.;
 #else
                 const double cj = v.c[j];
@@ -238,7 +239,7 @@ __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS)
 #if NK_PREFETCH
                 finish(j, g, xj, qj, lj, uj, aj);
 #else
-                finish(j, g, x[j], v.q[j], v.lb[j], v.ub[j], pending ? v.xa[j] : 0.);
+                finish(j, g, x[j], v.q ? v.q[j] : 0., v.lb[j], v.ub[j], pending ? v.xa[j] : 0.);
 #endif
             } else if constexpr (SPLIT) { // split region: the whole warp is here
                 int64_t j;
@@ -251,7 +252,7 @@ __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS)
                 if (done) {
                     if constexpr (FP32G)
                         g = v.c[j] + g;
-                    finish(j, g, x[j], v.q[j], v.lb[j], v.ub[j], pending ? v.xa[j] : 0.);
+                    finish(j, g, x[j], v.q ? v.q[j] : 0., v.lb[j], v.ub[j], pending ? v.xa[j] : 0.);
                 }
             }
         }

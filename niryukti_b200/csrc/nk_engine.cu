@@ -406,6 +406,7 @@ struct Engine {
     int64_t n = 0, m = 0;
     bool adaptive = false, halpern = false, residual_restarts = false, graphs = false;
     bool sparse_q = false, wide = false;
+    bool diag_q = false; // some q_j != 0 (an LP has none: the primal kernel skips q)
     int precision = NK_PRECISION_FP64;
     double reflection = 0, a_norm = 0, q_norm = 0;
     cudaStream_t stream = nullptr;
@@ -446,7 +447,7 @@ struct Engine {
     Vecs vecs() {
         Vecs v{};
         v.c = c.p;
-        v.q = q.p;
+        v.q = diag_q ? q.p : nullptr;
         v.lb = lb.p;
         v.ub = ub.p;
         v.rl = rl.p;
@@ -1273,6 +1274,7 @@ Engine *create_engine(const nk_csr *Ah, const nk_csr *Qh, const double *hc, cons
     };
     vec(E->c, hc, n, cperm);
     vec(E->q, hq, n, cperm);
+    E->diag_q = hq && std::any_of(hq, hq + n, [](double v) { return v != 0.; });
     vec(E->lb, hlb, n, cperm);
     vec(E->ub, hub, n, cperm);
     vec(E->rl, hrl, m, rperm);
