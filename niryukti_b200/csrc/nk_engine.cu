@@ -1892,6 +1892,8 @@ nk_status nk_batch_prepare(const nk_model *model, const nk_batch_options *o, nk_
         *out = nullptr;
         auto opts = batch_options(o);
         auto item = std::make_unique<nk_batch_item>();
+        // requests are prepared concurrently, one per host thread
+        nk::HostSerialScope serial;
         item->item = nk::batch_prepare(nk::host_model(model), opts);
         if (device_bytes)
             *device_bytes = item->item->decided ? 0. : double(item->item->bytes);

@@ -53,9 +53,16 @@ struct Accuracy { // vantage::Accuracy (include/vantage/vantage.hpp:78-82)
     bool finite = false;
 };
 
-// When set (per thread), host products run serially: callers that already run
-// one verifier per thread keep OpenMP from nesting teams inside them.
+// When set (per thread), host loops (presolve, scaling, verifier products) run
+// serially: callers that already run one model per thread keep OpenMP from
+// nesting teams inside them.
 void host_serial(bool serial);
+bool host_serial_enabled();
+struct HostSerialScope { // serial host loops on this thread until the scope ends
+    bool was;
+    HostSerialScope() : was(host_serial_enabled()) { host_serial(true); }
+    ~HostSerialScope() { host_serial(was); }
+};
 
 Csr build_csr(int64_t rows, int64_t cols, std::vector<Entry> e);
 Csr transpose(const Csr &a);

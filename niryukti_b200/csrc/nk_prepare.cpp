@@ -20,6 +20,9 @@
 namespace nk {
 namespace {
 constexpr double INF = std::numeric_limits<double>::infinity();
+// When set (per thread), host loops run serially: callers that already run
+// one presolve or verifier per thread keep OpenMP from nesting teams inside.
+thread_local bool g_host_serial = false;
 
 bool representable(double before, double after) {
     return std::isfinite(before) ? std::isfinite(after) && (before == 0 || after != 0)
@@ -27,9 +30,19 @@ bool representable(double before, double after) {
 }
 
 // extra_scale, src/preprocess.cpp:12-65 (reference built with VANTAGE_SPARSE_LU).
+//
+// Every loop below is element-wise (each row, column or entry is decided and
+// scaled from its own values), so the row-, column- and entry-parallel loops
+// compute exactly what the sequential ones do.  An entry that cannot take its
+// column's factor sets the column's factor to 1; the sequential loop reaches
+// the same verdict (once a column's factor is 1 every later entry takes it),
+// so the verdicts are gathered per column first and applied after.
 void extra_scale(Prepared &p, const std::vector<double> &row, std::vector<double> col) {
     HostModel &m = p.model;
-    for (size_t i = 0; i < row.size(); i++) {
+    const bool par = m.A.value.size() > 200000 && !g_host_serial;
+#pragma omp parallel for schedule(dynamic, 1024) if (par)
+    for (int64_t ii = 0; ii < int64_t(row.size()); ii++) {
+        const size_t i = size_t(ii);
         double f = row[i];
         bool safe = representable(p.row_scale[i], p.row_scale[i] * f) &&
                     representable(m.rl[i], m.rl[i] * f) && representable(m.ru[i], m.ru[i] * f);
@@ -43,18 +56,28 @@ void extra_scale(Prepared &p, const std::vector<double> &row, std::vector<double
         for (int64_t k = m.A.ptr[i]; k < m.A.ptr[i + 1]; k++)
             m.A.value[k] *= f;
     }
-    for (size_t j = 0; j < col.size(); j++) {
+#pragma omp parallel for if (par)
+    for (int64_t jj = 0; jj < int64_t(col.size()); jj++) {
+        const size_t j = size_t(jj);
         double f = col[j];
         if (!representable(p.column_scale[j], p.column_scale[j] * f) ||
             !representable(m.c[j], m.c[j] * f) || !representable(m.q[j], m.q[j] * (f * f)) ||
             !representable(m.lb[j], m.lb[j] / f) || !representable(m.ub[j], m.ub[j] / f))
             col[j] = 1;
     }
-    for (size_t k = 0; k < m.A.value.size(); k++) {
+    std::vector<unsigned char> refuse(col.size(), 0);
+#pragma omp parallel for if (par)
+    for (int64_t kk = 0; kk < int64_t(m.A.value.size()); kk++) {
+        const size_t k = size_t(kk);
         auto j = m.A.index[k];
-        if (!representable(m.A.value[k], m.A.value[k] * col[j]))
-            col[j] = 1;
+        if (!representable(m.A.value[k], m.A.value[k] * col[size_t(j)])) {
+#pragma omp atomic write
+            refuse[size_t(j)] = 1;
+        }
     }
+    for (size_t j = 0; j < col.size(); j++)
+        if (refuse[j])
+            col[j] = 1;
     bool qsafe = true;
     for (int64_t i = 0; i < m.Q.rows; ++i)
         for (auto k = m.Q.ptr[i]; k < m.Q.ptr[i + 1]; ++k)
@@ -64,7 +87,9 @@ void extra_scale(Prepared &p, const std::vector<double> &row, std::vector<double
     for (int64_t i = 0; i < m.Q.rows; ++i)
         for (auto k = m.Q.ptr[i]; k < m.Q.ptr[i + 1]; ++k)
             m.Q.value[k] *= col[i] * col[m.Q.index[k]];
-    for (size_t j = 0; j < col.size(); j++) {
+#pragma omp parallel for if (par)
+    for (int64_t jj = 0; jj < int64_t(col.size()); jj++) {
+        const size_t j = size_t(jj);
         double f = col[j];
         p.column_scale[j] *= f;
         m.c[j] *= f;
@@ -72,8 +97,9 @@ void extra_scale(Prepared &p, const std::vector<double> &row, std::vector<double
         m.lb[j] /= f;
         m.ub[j] /= f;
     }
-    for (size_t k = 0; k < m.A.value.size(); k++)
-        m.A.value[k] *= col[m.A.index[k]];
+#pragma omp parallel for if (par)
+    for (int64_t kk = 0; kk < int64_t(m.A.value.size()); kk++)
+        m.A.value[size_t(kk)] *= col[size_t(m.A.index[size_t(kk)])];
 }
 
 double geometric_factor(double low, double high) {
@@ -148,16 +174,53 @@ struct KeyHash {
         return size_t(h);
     }
 };
+
+// KeyHash of row [b, en) of A with its columns mapped, without building the key.
+uint64_t row_key_hash(const Csr &A, const std::vector<int64_t> &map, int64_t b, int64_t en) {
+    uint64_t h = 1469598103934665603ULL;
+    for (auto k = b; k < en; ++k) {
+        uint64_t bits;
+        std::memcpy(&bits, &A.value[size_t(k)], 8);
+        h = (h ^ uint64_t(map[size_t(A.index[size_t(k)])])) * 1099511628211ULL;
+        h = (h ^ bits) * 1099511628211ULL;
+    }
+    return h;
+}
+
+// Equal keys (mapped columns and values, in order) of source rows a and b --
+// the equality the reference's std::map of key vectors applies.
+bool same_row_key(const Csr &A, const std::vector<int64_t> &map, int64_t a, int64_t b) {
+    const int64_t ba = A.ptr[size_t(a)], ea = A.ptr[size_t(a + 1)];
+    const int64_t bb = A.ptr[size_t(b)], eb = A.ptr[size_t(b + 1)];
+    if (ea - ba != eb - bb)
+        return false;
+    for (int64_t t = 0; t < ea - ba; ++t)
+        if (map[size_t(A.index[size_t(ba + t)])] != map[size_t(A.index[size_t(bb + t)])] ||
+            !(A.value[size_t(ba + t)] == A.value[size_t(bb + t)]))
+            return false;
+    return true;
+}
 } // namespace
 
 // Sparse::build for entries that are already unique: sort (row, col), drop zeros.
 Csr build_csr(int64_t rows, int64_t cols, std::vector<Entry> e) {
-    std::sort(e.begin(), e.end(),
-              [](auto a, auto b) { return a.row < b.row || (a.row == b.row && a.col < b.col); });
+    auto before = [](const Entry &a, const Entry &b) {
+        return a.row < b.row || (a.row == b.row && a.col < b.col);
+    };
+    // Entries in strictly increasing (row, col) order -- the usual case, a CSR
+    // restricted to kept rows and columns -- have exactly one sorted order, so
+    // the sort is skipped; otherwise std::sort as in Sparse::build.
+    bool sorted = true;
+    for (size_t k = 1; k < e.size() && sorted; ++k)
+        sorted = before(e[k - 1], e[k]);
+    if (!sorted)
+        std::sort(e.begin(), e.end(), before);
     Csr s;
     s.rows = rows;
     s.cols = cols;
     s.ptr.assign(size_t(rows + 1), 0);
+    s.index.reserve(e.size());
+    s.value.reserve(e.size());
     for (size_t k = 0; k < e.size();) {
         auto a = e[k++];
         while (k < e.size() && e[k].row == a.row && e[k].col == a.col)
@@ -248,10 +311,19 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
         }
     const int64_t nk = int64_t(m.c.size());
     m.Q = build_csr(nk, nk, std::move(qe));
-    std::vector<Entry> e;
-    e.reserve(src.A.value.size());
-    std::unordered_map<std::vector<std::pair<int64_t, double>>, size_t, KeyHash> duplicate_rows;
+    // Rows in two passes.  The first, row-parallel, does each row's own
+    // arithmetic exactly as the reference's loop does (same operations, same
+    // order within the row): fixed-column shift, activity bounds, and the
+    // verdict (infeasible, dropped, or kept with bounds l, u), plus the hash of
+    // the row's key for duplicate detection.  The second walks the rows in
+    // order, so the first failure, the first occurrence of a duplicate key and
+    // the emitted order are the reference's.
+    enum : char { KEEP = 0, DROP = 1, FAIL_EMPTY = 2, FAIL_DISJOINT = 3 };
+    std::vector<char> verdict(size_t(mrows), KEEP), dupcand(size_t(mrows), 0);
+    std::vector<double> row_l(static_cast<size_t>(mrows)), row_u(static_cast<size_t>(mrows));
+    std::vector<uint64_t> key_hash(size_t(mrows), 0);
     const long double eps = std::numeric_limits<long double>::epsilon();
+#pragma omp parallel for schedule(dynamic, 1024) if (src.A.value.size() > 200000 && !g_host_serial)
     for (int64_t i = 0; i < mrows; i++) {
         long double shift = 0, shift_magnitude = 0;
         int64_t count = 0;
@@ -266,15 +338,18 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
                 count++;
         }
         double l = src.rl[i] - double(shift), u = src.ru[i] - double(shift);
+        row_l[size_t(i)] = l;
+        row_u[size_t(i)] = u;
         if (count == 0 && o.presolve) {
             long double guard = 8 * eps * (en - b + 1) * (1 + shift_magnitude);
             if (shift + guard < src.rl[i] || shift - guard > src.ru[i]) {
-                p.failure = "INFEASIBLE";
-                p.reason = "Empty row after fixed-variable substitution: r" + std::to_string(i);
-                return p;
-            }
-            if (l <= 0 && u >= 0)
+                verdict[size_t(i)] = FAIL_EMPTY;
                 continue;
+            }
+            if (l <= 0 && u >= 0) {
+                verdict[size_t(i)] = DROP;
+                continue;
+            }
         }
         long double amin = 0, amax = 0, magnitude = 0;
         for (auto k = b; k < en; k++) {
@@ -289,24 +364,49 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
             long double slack = 8 * eps * (en - b + 1) * (1 + magnitude);
             if (std::isfinite(amin) && std::isfinite(amax) &&
                 (amin > src.ru[i] + slack || amax < src.rl[i] - slack)) {
-                p.failure = "INFEASIBLE";
-                p.reason = "Verified disjoint row activity bounds: r" + std::to_string(i);
-                return p;
+                verdict[size_t(i)] = FAIL_DISJOINT;
+                continue;
             }
         }
         if (o.presolve && std::isfinite(amin) && std::isfinite(amax)) {
             long double guard = 8 * eps * (en - b + 1) * (1 + magnitude);
-            if (amin - guard >= src.rl[i] && amax + guard <= src.ru[i])
+            if (amin - guard >= src.rl[i] && amax + guard <= src.ru[i]) {
+                verdict[size_t(i)] = DROP;
                 continue;
+            }
         }
         if (o.presolve && count == en - b) {
-            std::vector<std::pair<int64_t, double>> key;
-            key.reserve(size_t(en - b));
-            for (auto k = b; k < en; ++k)
-                key.push_back({map[size_t(src.A.index[size_t(k)])], src.A.value[size_t(k)]});
-            auto found = duplicate_rows.find(key);
-            if (found != duplicate_rows.end()) {
-                auto r = found->second;
+            dupcand[size_t(i)] = 1;
+            key_hash[size_t(i)] = row_key_hash(src.A, map, b, en);
+        }
+    }
+    // first occurrence (prepared row) of each key, by hash; keys are compared in full
+    std::unordered_multimap<uint64_t, size_t> duplicate_rows;
+    size_t kept_entries = 0;
+    for (int64_t i = 0; i < mrows; i++) {
+        const char v = verdict[size_t(i)];
+        if (v == FAIL_EMPTY) {
+            p.failure = "INFEASIBLE";
+            p.reason = "Empty row after fixed-variable substitution: r" + std::to_string(i);
+            return p;
+        }
+        if (v == FAIL_DISJOINT) {
+            p.failure = "INFEASIBLE";
+            p.reason = "Verified disjoint row activity bounds: r" + std::to_string(i);
+            return p;
+        }
+        if (v == DROP)
+            continue;
+        const double l = row_l[size_t(i)], u = row_u[size_t(i)];
+        const int64_t b = src.A.ptr[size_t(i)], en = src.A.ptr[size_t(i + 1)];
+        if (dupcand[size_t(i)]) {
+            const uint64_t h = key_hash[size_t(i)];
+            bool merged = false;
+            auto range = duplicate_rows.equal_range(h);
+            for (auto it = range.first; it != range.second; ++it) {
+                const size_t r = it->second;
+                if (!same_row_key(src.A, map, p.rows[r], i))
+                    continue;
                 if (l > m.rl[r]) {
                     m.rl[r] = l;
                     p.lower_rows[r] = i;
@@ -325,19 +425,28 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
                         p.failure_ray.clear();
                     return p;
                 }
-                continue;
+                merged = true;
+                break;
             }
-            duplicate_rows.emplace(std::move(key), p.rows.size());
+            if (merged)
+                continue;
+            duplicate_rows.emplace(h, p.rows.size());
         }
-        auto row = int64_t(p.rows.size());
         p.rows.push_back(i);
         p.lower_rows.push_back(i);
         p.upper_rows.push_back(i);
         m.rl.push_back(l);
         m.ru.push_back(u);
         for (auto k = b; k < en; k++)
+            kept_entries += map[size_t(src.A.index[size_t(k)])] >= 0;
+    }
+    std::vector<Entry> e;
+    e.reserve(kept_entries);
+    for (size_t r = 0; r < p.rows.size(); ++r) {
+        const int64_t i = p.rows[r];
+        for (auto k = src.A.ptr[size_t(i)]; k < src.A.ptr[size_t(i + 1)]; k++)
             if (map[size_t(src.A.index[size_t(k)])] >= 0)
-                e.push_back({row, map[size_t(src.A.index[size_t(k)])], src.A.value[size_t(k)]});
+                e.push_back({int64_t(r), map[size_t(src.A.index[size_t(k)])], src.A.value[size_t(k)]});
     }
     m.A = build_csr(int64_t(m.rl.size()), nk, std::move(e));
     p.column_scale.assign(size_t(nk), 1);
@@ -346,16 +455,31 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
         geometric_scale(p);
     for (int pass = 0; pass < o.scaling_passes; pass++) {
         std::vector<double> row(m.rl.size(), 1), col(m.c.size(), 1);
-        for (size_t i = 0; i < row.size(); ++i) {
+        const bool par = m.A.value.size() > 200000 && !g_host_serial;
+#pragma omp parallel for schedule(dynamic, 1024) if (par)
+        for (int64_t ii = 0; ii < int64_t(row.size()); ++ii) {
+            const size_t i = size_t(ii);
             double norm = 0;
             for (auto k = m.A.ptr[i]; k < m.A.ptr[i + 1]; ++k)
                 norm = std::max(norm, std::abs(m.A.value[size_t(k)]));
             row[i] = norm > 0 ? std::clamp(1 / std::sqrt(norm), 1e-3, 1e3) : 1.;
         }
         extra_scale(p, row, col);
+        // column maxima: a maximum does not depend on the order it is taken in,
+        // and the bits of non-negative doubles order like their values
         std::vector<double> norm(col.size());
-        for (size_t k = 0; k < m.A.value.size(); ++k)
-            norm[size_t(m.A.index[k])] = std::max(norm[size_t(m.A.index[k])], std::abs(m.A.value[k]));
+#pragma omp parallel for if (par)
+        for (int64_t kk = 0; kk < int64_t(m.A.value.size()); ++kk) {
+            const size_t k = size_t(kk);
+            const double v = std::abs(m.A.value[k]);
+            uint64_t bits, *slot = reinterpret_cast<uint64_t *>(&norm[size_t(m.A.index[k])]);
+            std::memcpy(&bits, &v, 8);
+            uint64_t cur = __atomic_load_n(slot, __ATOMIC_RELAXED);
+            while (bits > cur &&
+                   !__atomic_compare_exchange_n(slot, &cur, bits, true, __ATOMIC_RELAXED,
+                                                __ATOMIC_RELAXED)) {
+            }
+        }
         for (size_t j = 0; j < col.size(); ++j)
             col[j] = norm[j] > 0 ? std::clamp(1 / std::sqrt(norm[j]), 1e-3, 1e3) : 1.;
         std::fill(row.begin(), row.end(), 1);
@@ -401,7 +525,6 @@ namespace {
 long double down(long double v) { return std::nextafter(v, -std::numeric_limits<long double>::infinity()); }
 long double up(long double v) { return std::nextafter(v, std::numeric_limits<long double>::infinity()); }
 bool has_q(const HostModel &m) { return !m.Q.value.empty(); }
-thread_local bool g_host_serial = false;
 
 std::vector<double> multiply(const Csr &a, const std::vector<double> &x) {
     std::vector<double> y(size_t(a.rows));
@@ -495,6 +618,7 @@ double lp_lower_bound(const HostModel &m, const Csr &at, const std::vector<doubl
 } // namespace
 
 void host_serial(bool serial) { g_host_serial = serial; }
+bool host_serial_enabled() { return g_host_serial; }
 
 bool HostModel::is_qp() const {
     return !Q.value.empty() || std::any_of(q.begin(), q.end(), [](double v) { return v != 0; });

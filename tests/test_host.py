@@ -87,22 +87,22 @@ def presolve_qp():
     return m
 
 
-def random_presolve_model(seed):
+def random_presolve_model(seed, m=300, n=700, per_col=4, fixed=40, dups=25, redundant=10):
     """A random LP with fixed columns, duplicated and redundant rows."""
-    base = synth.random_lp(m=300, n=700, per_col=4, seed=seed)
+    base = synth.random_lp(m=m, n=n, per_col=per_col, seed=seed)
     rng = np.random.default_rng(seed)
     lb, ub = base.lb.copy(), base.ub.copy()
-    fixed = rng.choice(base.n, 40, replace=False)
+    fixed = rng.choice(base.n, fixed, replace=False)
     lb[fixed] = ub[fixed] = base.x0[fixed]
     rows = [list(zip(base.idx[base.ptr[i]:base.ptr[i + 1]].tolist(),
                      base.val[base.ptr[i]:base.ptr[i + 1]].tolist())) for i in range(base.m)]
     rl, ru = base.rl.tolist(), base.ru.tolist()
-    for i in rng.choice(base.m, 25, replace=False):     # duplicates with looser/tighter bounds
+    for i in rng.choice(base.m, dups, replace=False):   # duplicates with looser/tighter bounds
         rows.append(rows[i])
         slack = float(rng.uniform(0, 1))
         rl.append(rl[i] - slack)
         ru.append(ru[i] + slack)
-    for _ in range(10):                                   # redundant rows
+    for _ in range(redundant):                            # redundant rows
         cols = rng.choice(base.n, 3, replace=False)
         rows.append([(int(j), 1e-4) for j in cols])
         rl.append(-1.0)
@@ -149,6 +149,25 @@ def test_prepare_bit_exact(reference, name, opts):
         same(mine[key], ref[key], key)
     same([mine["objective_scale"], mine["offset"]], [ref["objective_scale"], ref["offset"]],
          "scalars")
+
+
+@pytest.mark.parametrize("opts", OPTIONS[:2], ids=["presolve", "no-presolve"])
+def test_prepare_bit_exact_threaded(reference, opts):
+    """Above 200,000 nonzeros the row pass and the scaling loops run on all
+    host threads; the prepared model must still be the reference's, bit for
+    bit (fixed columns, duplicated and redundant rows included)."""
+    model = random_presolve_model(21, m=30000, n=70000, per_col=6, fixed=4000, dups=2500,
+                                  redundant=1000)
+    assert model.nnz > 200000
+    mine = solver.prepare(model, **opts)
+    ref = reference.model(model).prepare(**opts)
+    for key in ("ptr", "idx", "val", "c", "lb", "ub", "rl", "ru", "cols", "rows", "lower_rows",
+                "upper_rows", "fixed", "column_scale", "row_scale"):
+        same(mine[key], ref[key], key)
+    same([mine["objective_scale"], mine["offset"]], [ref["objective_scale"], ref["offset"]],
+         "scalars")
+    if opts["presolve"]:
+        assert len(mine["rows"]) < model.m  # the presolve rules did remove rows
 
 
 def test_presolve_rules_fire(reference):
