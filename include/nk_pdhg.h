@@ -272,6 +272,13 @@ nk_status nk_batch_estimate(const nk_model *model, double *bytes);
  * *device_bytes: what admitting it will take (0 if it terminated already). */
 nk_status nk_batch_prepare(const nk_model *model, const nk_batch_options *options,
                            nk_batch_item **out, double *device_bytes);
+/* nk_batch_prepare with a start point: x0 (n) and y0 (m) in the caller's
+ * order (either may be NULL), taken like Options::initial_x / initial_y.  It
+ * serves the warm-started box variants of cuda_batch_relaxations
+ * (src/cuda.cu:1136-1160; caller src/mip.cpp:1094-1118). */
+nk_status nk_batch_prepare_from(const nk_model *model, const nk_batch_options *options,
+                                const double *x0, const double *y0, nk_batch_item **out,
+                                double *device_bytes);
 void nk_batch_item_free(nk_batch_item *item);
 /* Admits a prepared instance under `id`: *admitted = 1 (the batch owns the
  * item now) or 0 (over the memory budget or no free slot; the caller keeps it). */

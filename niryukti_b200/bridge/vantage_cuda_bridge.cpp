@@ -10,13 +10,18 @@
 // reference's convention (src/cuda.cu:10-17), so the driver's automatic CPU
 // fallback on memory-guard failures (src/solver.cpp:356-367) keeps working.
 //
-// The side entries of the CUDA build that are not part of the PDHG path
-// (cuda_batch_relaxations, cuda_linear_solve, cuda_propagate_integer_bounds,
-// cuda_compact_matrix) report that the B200 engine does not provide them,
+// cuda_batch_relaxations (the box variants of one LP relaxation that the
+// branch-and-bound driver scores for strong branching) runs on the engine's
+// batched solver.  The other side entries of the CUDA build, which are not
+// part of the PDHG path (cuda_linear_solve, cuda_propagate_integer_bounds,
+// cuda_compact_matrix), report that the B200 engine does not provide them,
 // exactly where a CPU build reports that CUDA is missing.
 #include "internal.hpp"
 #include "nk_pdhg.h"
 
+#include <algorithm>
+#include <chrono>
+#include <cmath>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -175,10 +180,118 @@ bool cuda_propagate_integer_bounds(const Model &, std::vector<double> &, std::ve
                                    int) {
     throw std::runtime_error("GPU propagation is not provided by the B200 PDHG engine");
 }
-std::vector<Result> cuda_batch_relaxations(const Model &, const std::vector<std::vector<double>> &,
-                                           const std::vector<std::vector<double>> &,
-                                           const Options &) {
-    throw std::runtime_error("Batched relaxations are not provided by the B200 PDHG engine");
+// cuda_batch_relaxations (src/cuda.cu:1136-1266): the same argument checks,
+// start point (initial_x clamped into each box, initial_y), limits and result
+// fields as the reference.  Where the reference advances all boxes with one
+// fixed-step PDHG and keeps the better of the average and the current point,
+// each box here is an instance of the engine's batch -- its own presolve,
+// scaling, adaptive steps and restarts, FP64 matrices -- and returns its best
+// point.  Either way the box's status comes from the reference's own
+// verify(child, x, y): OPTIMAL when the KKT error is within tol, else the limit
+// that ended the run.
+std::vector<Result> cuda_batch_relaxations(const Model &m,
+                                           const std::vector<std::vector<double>> &lower,
+                                           const std::vector<std::vector<double>> &upper,
+                                           const Options &o) {
+    m.validate();
+    if (m.is_qp() || m.is_mip() || lower.empty() || lower.size() != upper.size() ||
+        lower.size() > 32 || m.c.empty())
+        throw std::runtime_error("Invalid CUDA LP relaxation batch");
+    using Clock = std::chrono::steady_clock;
+    const auto start = Clock::now();
+    auto elapsed = [&] { return std::chrono::duration<double>(Clock::now() - start).count(); };
+    const size_t n = m.c.size(), rows = m.rl.size(), boxes = lower.size();
+    for (size_t b = 0; b < boxes; ++b) {
+        if (lower[b].size() != n || upper[b].size() != n)
+            throw std::runtime_error("Batch bound dimensions");
+        for (size_t j = 0; j < n; ++j)
+            if (std::isnan(lower[b][j]) || std::isnan(upper[b][j]) || lower[b][j] > upper[b][j] ||
+                lower[b][j] < m.lb[j] || upper[b][j] > m.ub[j])
+                throw std::runtime_error("Invalid batch bounds");
+    }
+    nk_batch_options bo;
+    nk_batch_defaults(&bo);
+    bo.tol = o.tol;
+    bo.time_limit = o.time_limit;
+    bo.iteration_limit = o.iteration_limit;
+    bo.check_every = o.check_every;
+    bo.presolve = o.presolve;
+    bo.scaling_combined = o.scaling == "combined";
+    bo.scaling_passes = o.scaling_passes;
+    bo.adaptive = o.adaptive;
+    bo.restart = o.restart;
+    bo.graphs = o.cuda_graphs;
+    bo.precision = NK_PRECISION_FP64;
+    nk_batch *batch = nullptr;
+    check(nk_batch_create(&bo, &batch));
+    struct Closer {
+        nk_batch *b;
+        ~Closer() { nk_batch_destroy(b); }
+    } closer{batch};
+    nk_csr a{m.A.rows, m.A.cols, m.A.ptr.data(), m.A.index.data(), m.A.value.data()};
+    nk_csr noq{0, 0, nullptr, nullptr, nullptr};
+    std::vector<double> x0(n);
+    for (size_t b = 0; b < boxes; ++b) {
+        nk_model child{a, noq, m.c.data(), m.q.size() == n ? m.q.data() : nullptr, lower[b].data(), upper[b].data(),
+                       m.rl.data(), m.ru.data(), m.offset};
+        for (size_t j = 0; j < n; ++j)
+            x0[j] = std::clamp(o.initial_x.empty() ? 0 : o.initial_x.at(j), lower[b][j],
+                               upper[b][j]);
+        if (!o.initial_y.empty() && o.initial_y.size() != rows)
+            throw std::runtime_error("Batch initial dual dimensions");
+        nk_batch_item *item = nullptr;
+        double bytes = 0;
+        check(nk_batch_prepare_from(&child, &bo, x0.data(),
+                                    o.initial_y.empty() ? nullptr : o.initial_y.data(), &item,
+                                    &bytes));
+        int admitted = 0;
+        nk_status st = nk_batch_admit(batch, item, int64_t(b), &admitted);
+        if (st != NK_OK || !admitted) {
+            nk_batch_item_free(item);
+            if (st != NK_OK)
+                check(st);
+            throw std::runtime_error("GPU relaxation batch exceeds available memory");
+        }
+    }
+    std::vector<Result> results(boxes);
+    std::vector<int64_t> finished(boxes);
+    size_t collected = 0;
+    std::vector<double> x(n), y(rows);
+    while (collected < boxes) {
+        int count = 0;
+        check(nk_batch_step(batch, 1 << 30, finished.data(), int(finished.size()), &count));
+        for (int k = 0; k < count; ++k) {
+            const size_t b = size_t(finished[size_t(k)]);
+            nk_solve_result sr{};
+            check(nk_batch_result(batch, int64_t(b), &sr, x.data(), y.data()));
+            Model child = m;
+            child.lb = lower[b];
+            child.ub = upper[b];
+            Result &r = results[b];
+            r.backend = gpu_backend_name();
+            r.device_name = cuda_description();
+            r.method_selected = "batched-pdhg";
+            r.x = x;
+            r.y = y;
+            r.accuracy = verify(child, r.x, r.y);
+            r.status = r.accuracy.finite && r.accuracy.kkt <= o.tol ? "OPTIMAL"
+                       : stop_requested(o)                          ? "INTERRUPTED"
+                       : elapsed() >= o.time_limit                  ? "TIME_LIMIT"
+                                                                    : "ITERATION_LIMIT";
+            r.iterations = sr.iterations;
+            r.restarts = sr.restarts;
+            r.rejected_steps = sr.rejected_steps;
+            r.preprocess_seconds = sr.preprocess_seconds;
+            r.iteration_seconds = sr.iteration_seconds;
+            r.verification_seconds = sr.verification_seconds;
+            ++collected;
+        }
+        if (count == 0 && collected < boxes)
+            throw std::runtime_error("GPU relaxation batch stopped without finishing");
+    }
+    for (auto &r : results)
+        r.seconds = elapsed();
+    return results;
 }
 std::vector<double> cuda_linear_solve(const Sparse &, const std::vector<double> &,
                                       const Options &, bool, double) {

@@ -119,7 +119,11 @@ inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
 // Prepares one instance for a batch: everything solve() does before the first
 // iteration, plus the instance's SELL layout.  Thread-safe (no device calls).
-inline std::unique_ptr<BatchItem> batch_prepare(const HostModel &original, const BatchOptions &o) {
+// x0 / y0 (optional, the caller's n and m entries): the start point, taken into
+// the prepared space as nk_solve takes Options::initial_x / initial_y.
+inline std::unique_ptr<BatchItem> batch_prepare(const HostModel &original, const BatchOptions &o,
+                                                const std::vector<double> *x0 = nullptr,
+                                                const std::vector<double> *y0 = nullptr) {
     using namespace batch_detail;
     auto it = std::make_unique<BatchItem>();
     BatchItem &B = *it;
@@ -150,8 +154,15 @@ inline std::unique_ptr<BatchItem> batch_prepare(const HostModel &original, const
     R.removed_columns = int64_t(B.orig.c.size()) - B.n;
     R.removed_rows = int64_t(B.orig.rl.size()) - B.m;
     std::vector<double> x(static_cast<size_t>(B.n)), y(static_cast<size_t>(B.m));
-    for (int64_t j = 0; j < B.n; j++)
-        x[size_t(j)] = std::clamp(0.0, pm.lb[size_t(j)], pm.ub[size_t(j)]);
+    for (int64_t j = 0; j < B.n; j++) {
+        const double initial = x0 ? (*x0)[size_t(B.prep.cols[size_t(j)])] : 0.;
+        x[size_t(j)] = std::clamp(initial / B.prep.column_scale[size_t(j)], pm.lb[size_t(j)],
+                                  pm.ub[size_t(j)]);
+    }
+    if (y0)
+        for (int64_t i = 0; i < B.m; i++)
+            y[size_t(i)] = (*y0)[size_t(B.prep.rows[size_t(i)])] /
+                           (B.prep.row_scale[size_t(i)] * B.prep.objective_scale);
     R.x = B.prep.restore_x(x);
     R.y = B.prep.restore_y(y, B.orig.rl.size());
     R.accuracy = B.verifier->evaluate(R.x, R.y);

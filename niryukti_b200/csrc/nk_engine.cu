@@ -1900,6 +1900,28 @@ nk_status nk_batch_prepare(const nk_model *model, const nk_batch_options *o, nk_
         *out = item.release();
     });
 }
+nk_status nk_batch_prepare_from(const nk_model *model, const nk_batch_options *o,
+                                const double *x0, const double *y0, nk_batch_item **out,
+                                double *device_bytes) {
+    return guard([&] {
+        if (!out)
+            throw nk::Error(NK_ERR_INVALID, "null output handle");
+        *out = nullptr;
+        auto opts = batch_options(o);
+        auto host = nk::host_model(model);
+        std::vector<double> x, y;
+        if (x0)
+            x.assign(x0, x0 + host.c.size());
+        if (y0)
+            y.assign(y0, y0 + host.rl.size());
+        auto item = std::make_unique<nk_batch_item>();
+        nk::HostSerialScope serial;
+        item->item = nk::batch_prepare(host, opts, x0 ? &x : nullptr, y0 ? &y : nullptr);
+        if (device_bytes)
+            *device_bytes = item->item->decided ? 0. : double(item->item->bytes);
+        *out = item.release();
+    });
+}
 void nk_batch_item_free(nk_batch_item *item) { delete item; }
 
 nk_status nk_batch_admit(nk_batch *h, nk_batch_item *item, int64_t id, int *admitted) {

@@ -292,6 +292,8 @@ class Reference:
         L.ref_prepared_get.argtypes = [C.c_void_p, _I, _I, _D, _D, _D, _D, _D, _D, _D, _I, _I,
                                        _I, _I, _D, _D, _D, _D, _I, _I, _D]
         L.ref_cuda_available.restype = C.c_int
+        L.ref_batch_relaxations.argtypes = [C.c_void_p, C.c_int, _D, _D, _D, _D, C.c_char_p, _D,
+                                            C.POINTER(C.c_int), _D, _D]
 
     def error(self):
         return self.lib.ref_last_error().decode()
@@ -360,6 +362,32 @@ class RefModel:
         r["status"] = status.value.decode()
         r["x"], r["y"] = x, y
         return r
+
+    def batch_relaxations(self, lower, upper, x0=None, y0=None, **opts):
+        """cuda_batch_relaxations(model, lower, upper, options): one result per box."""
+        lower = np.ascontiguousarray(lower, dtype=np.float64)
+        upper = np.ascontiguousarray(upper, dtype=np.float64)
+        boxes = lower.shape[0]
+        st = np.zeros(10 * boxes)
+        status = (C.c_int * boxes)()
+        xs, ys = np.zeros(boxes * self.n), np.zeros(boxes * self.m)
+        x0 = None if x0 is None else np.ascontiguousarray(x0, dtype=np.float64)
+        y0 = None if y0 is None else np.ascontiguousarray(y0, dtype=np.float64)
+        rc = self.r.lib.ref_batch_relaxations(self.h, boxes, _d(lower), _d(upper),
+                                               None if x0 is None else _d(x0),
+                                               None if y0 is None else _d(y0), _kv(opts),
+                                               _d(st), status, _d(xs), _d(ys))
+        if rc != 0:
+            raise RuntimeError(self.r.error())
+        names = ("OPTIMAL", "INTERRUPTED", "TIME_LIMIT", "ITERATION_LIMIT", "OTHER")
+        out = []
+        for b in range(boxes):
+            s = st[10 * b:10 * b + 10]
+            out.append({"status": names[status[b]], "objective": s[0], "kkt": s[1],
+                        "finite": bool(s[2]), "iterations": int(s[3]), "restarts": int(s[4]),
+                        "seconds": s[5], "x": xs[b * self.n:(b + 1) * self.n],
+                        "y": ys[b * self.m:(b + 1) * self.m]})
+        return out
 
     def verify(self, x, y, safe=True):
         acc = np.zeros(10)

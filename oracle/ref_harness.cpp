@@ -372,4 +372,48 @@ void ref_prepared_get(ref_prepared *h, int64_t *ptr, int64_t *idx, double *val, 
     cp(qval, m.Q.value);
 }
 int ref_cuda_available(void) { return cuda_available() ? 1 : 0; }
+
+// cuda_batch_relaxations(model, lower, upper, options) -- src/internal.hpp:60-62.
+// lower / upper: `boxes` rows of n bounds; x0 / y0 (may be NULL) become
+// Options::initial_x / initial_y.  Per box, stats[10 * b ...] = [objective,
+// kkt, finite, iterations, restarts, seconds, 0, 0, 0, 0], status[b] in
+// {0 OPTIMAL, 1 INTERRUPTED, 2 TIME_LIMIT, 3 ITERATION_LIMIT, 4 other}; x_out
+// (boxes * n) and y_out (boxes * m) may be NULL.
+int ref_batch_relaxations(ref_model *r, int boxes, const double *lower, const double *upper,
+                          const double *x0, const double *y0, const char *opts, double *stats,
+                          int *status, double *x_out, double *y_out) {
+    try {
+        auto o = make_options(opts);
+        const size_t n = r->m.c.size(), m = r->m.rl.size();
+        if (x0)
+            o.initial_x.assign(x0, x0 + n);
+        if (y0)
+            o.initial_y.assign(y0, y0 + m);
+        std::vector<std::vector<double>> lo(static_cast<size_t>(boxes)), up(static_cast<size_t>(boxes));
+        for (int b = 0; b < boxes; ++b) {
+            lo[size_t(b)].assign(lower + size_t(b) * n, lower + size_t(b + 1) * n);
+            up[size_t(b)].assign(upper + size_t(b) * n, upper + size_t(b + 1) * n);
+        }
+        auto res = cuda_batch_relaxations(r->m, lo, up, o);
+        for (size_t b = 0; b < res.size(); ++b) {
+            const auto &q = res[b];
+            double s[10] = {q.accuracy.objective, q.accuracy.kkt, q.accuracy.finite ? 1. : 0.,
+                            double(q.iterations), double(q.restarts), q.seconds, 0, 0, 0, 0};
+            std::memcpy(stats + 10 * b, s, sizeof(s));
+            status[b] = q.status == "OPTIMAL"           ? 0
+                        : q.status == "INTERRUPTED"     ? 1
+                        : q.status == "TIME_LIMIT"      ? 2
+                        : q.status == "ITERATION_LIMIT" ? 3
+                                                        : 4;
+            if (x_out && q.x.size() == n)
+                std::memcpy(x_out + b * n, q.x.data(), n * sizeof(double));
+            if (y_out && q.y.size() == m)
+                std::memcpy(y_out + b * m, q.y.data(), m * sizeof(double));
+        }
+        return 0;
+    } catch (const std::exception &e) {
+        set_error(e.what());
+        return -1;
+    }
+}
 }

@@ -60,3 +60,57 @@ def test_bridged_solve_mixed_precision(bridged):
                                    cuda_graphs=True, iteration_limit=200000)
     assert r["status"] == "OPTIMAL" and r["kkt"] <= 1e-6
     assert abs(r["objective"] - want["objective"]) <= 2e-6 * (1 + abs(want["objective"]))
+
+
+def _branching_boxes(model, x, count=4):
+    """Down and up boxes of the first `count` columns that sit strictly inside
+    their bounds at a fractional value -- the shortlist the reference's
+    branch-and-bound scores (src/mip.cpp:1094-1118)."""
+    frac = np.where((x > model.lb + 0.2) & (x < model.ub - 0.2) &
+                    (np.abs(x - np.round(x)) > 0.2))[0][:count]
+    lows, ups = [], []
+    for j in frac:
+        for up in (False, True):
+            lo, hi = model.lb.copy(), model.ub.copy()
+            if up:
+                lo[j] = np.ceil(x[j])
+            else:
+                hi[j] = np.floor(x[j])
+            lows.append(lo)
+            ups.append(hi)
+    return np.array(lows), np.array(ups)
+
+
+def test_bridged_batch_relaxations(bridged, reference):
+    """cuda_batch_relaxations through the bridge: eight strong-branching boxes
+    of one LP, warm-started from the parent's solution, solved together by the
+    engine's batch.  Every box must come back OPTIMAL under the reference's own
+    verify(), with the objective of the reference's CPU solve of that box
+    (within 2 tol (1 + |f|))."""
+    import copy
+    model = synth.random_lp(m=300, n=700, per_col=4, seed=3)
+    parent = reference.model(model).solve(method="pdhg", device="cpu", iteration_limit=200000)
+    assert parent["status"] == "OPTIMAL"
+    lows, ups = _branching_boxes(model, parent["x"])
+    assert len(lows) == 8
+    got = bridged.model(model).batch_relaxations(lows, ups, x0=parent["x"], y0=parent["y"],
+                                                 tol=1e-6, iteration_limit=200000,
+                                                 time_limit=120)
+    for b, r in enumerate(got):
+        child = copy.copy(model)
+        child.lb, child.ub = lows[b], ups[b]
+        want = reference.model(child).solve(method="pdhg", device="cpu", iteration_limit=200000)
+        assert want["status"] == "OPTIMAL"
+        assert r["status"] == "OPTIMAL" and r["kkt"] <= 1e-6, (b, r["status"], r["kkt"])
+        assert abs(r["objective"] - want["objective"]) <= 2e-6 * (1 + abs(want["objective"]))
+        # the returned point is the box's own: within its bounds
+        assert np.all(r["x"] >= lows[b] - 1e-9) and np.all(r["x"] <= ups[b] + 1e-9)
+
+
+def test_bridged_batch_relaxations_checks_bounds(bridged):
+    """The reference's argument checks: a box outside the model's bounds is refused."""
+    model = synth.random_lp(m=300, n=700, per_col=4, seed=3)
+    lo, hi = model.lb.copy()[None, :], model.ub.copy()[None, :]
+    hi[0, 5] = model.ub[5] + 1.0
+    with pytest.raises(RuntimeError, match="Invalid batch bounds"):
+        bridged.model(model).batch_relaxations(lo, hi, tol=1e-6)

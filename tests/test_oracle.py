@@ -232,3 +232,11 @@ def test_oracle_infeasibility_bound(oracle, reference):
     a = oracle.model(m).infeasibility_bound(ray)
     b = reference.model(m).infeasibility_bound(ray)
     assert a == b and a > 0
+
+
+def test_reference_cpu_build_has_no_batched_relaxations(reference):
+    """The harness reaches cuda_batch_relaxations; in the reference's CPU build
+    it is the stub that asks for a CUDA build (src/cuda_stub.cpp:13-17)."""
+    model = synth.random_lp(m=50, n=120, per_col=3, seed=2)
+    with pytest.raises(RuntimeError, match="require a CUDA build"):
+        reference.model(model).batch_relaxations(model.lb[None, :], model.ub[None, :], tol=1e-6)
