@@ -338,6 +338,20 @@ nk_status nk_monitor_static(int64_t n, int64_t m, const double *x, const double 
                             const double *rl, const double *ru, double cscale, double *result,
                             void *stream);
 
+/* cuda_compact_matrix(matrix, rows, columns, output_columns) -- src/cuda.cu:953-1032,
+ * called by prepare with --gpu-presolve (src/preprocess.cpp:295-298).  The CSR
+ * of the kept rows (kept_rows: `rows` strictly increasing source rows) with the
+ * kept columns renumbered (column_map: one entry per source column, -1 drops
+ * it, the kept ones strictly increasing below output_columns), entries in
+ * their source order.  Host arrays in and out: out_ptr has rows + 1 entries,
+ * out_index / out_value `capacity` (at most the kept rows' entries are
+ * needed); *out_nnz receives the kept entries.  Counted, scanned and compacted
+ * on the GPU. */
+nk_status nk_compact_csr(const nk_csr *matrix, int64_t rows, const int64_t *kept_rows,
+                         const int64_t *column_map, int64_t output_columns, int64_t *out_ptr,
+                         int64_t *out_index, double *out_value, int64_t capacity,
+                         int64_t *out_nnz);
+
 int nk_cuda_available(void);
 nk_status nk_cuda_description(char *buffer, int length);
 nk_status nk_hardware_info(int *available, double *free_bytes, double *total_bytes);

@@ -12,15 +12,17 @@
 //
 // cuda_batch_relaxations (the box variants of one LP relaxation that the
 // branch-and-bound driver scores for strong branching) runs on the engine's
-// batched solver.  The other side entries of the CUDA build, which are not
-// part of the PDHG path (cuda_linear_solve, cuda_propagate_integer_bounds,
-// cuda_compact_matrix), report that the B200 engine does not provide them,
-// exactly where a CPU build reports that CUDA is missing.
+// batched solver, and cuda_compact_matrix (prepare's CSR step under
+// --gpu-presolve) on its compaction kernels.  The other side entries of the
+// CUDA build, which are not part of the PDHG path (cuda_linear_solve,
+// cuda_propagate_integer_bounds), report that the B200 engine does not provide
+// them, exactly where a CPU build reports that CUDA is missing.
 #include "internal.hpp"
 #include "nk_pdhg.h"
 
 #include <algorithm>
 #include <chrono>
+#include <climits>
 #include <cmath>
 #include <stdexcept>
 #include <string>
@@ -172,9 +174,47 @@ std::string cuda_description() {
     return buffer;
 }
 
-Sparse cuda_compact_matrix(const Sparse &, const std::vector<int64_t> &,
-                           const std::vector<int64_t> &, int64_t) {
-    throw std::runtime_error("GPU matrix compaction is not provided by the B200 PDHG engine");
+// cuda_compact_matrix (src/cuda.cu:978-1032), the CSR step of prepare with
+// --gpu-presolve: the reference's argument checks and messages, then the
+// engine's count / scan / ordered-scatter compaction (nk_compact_csr).
+Sparse cuda_compact_matrix(const Sparse &matrix, const std::vector<int64_t> &rows,
+                           const std::vector<int64_t> &columns, int64_t output_columns) {
+    if (columns.size() != size_t(matrix.cols) || output_columns < 0 || rows.size() >= INT_MAX)
+        throw std::runtime_error("GPU compaction dimensions");
+    int64_t previous = -1;
+    for (auto row : rows) {
+        if (row <= previous || row >= matrix.rows)
+            throw std::runtime_error("GPU compaction row map");
+        previous = row;
+    }
+    previous = -1;
+    for (auto column : columns)
+        if (column >= 0) {
+            if (column <= previous || column >= output_columns)
+                throw std::runtime_error("GPU compaction column map");
+            previous = column;
+        }
+    Sparse result;
+    result.rows = int64_t(rows.size());
+    result.cols = output_columns;
+    if (rows.empty()) {
+        result.ptr = {0};
+        return result;
+    }
+    int64_t capacity = 0;
+    for (auto row : rows)
+        capacity += matrix.ptr[size_t(row + 1)] - matrix.ptr[size_t(row)];
+    result.ptr.resize(rows.size() + 1);
+    result.index.resize(size_t(capacity));
+    result.value.resize(size_t(capacity));
+    nk_csr a{matrix.rows, matrix.cols, matrix.ptr.data(), matrix.index.data(), matrix.value.data()};
+    int64_t kept = 0;
+    check(nk_compact_csr(&a, int64_t(rows.size()), rows.data(), columns.data(), output_columns,
+                         result.ptr.data(), result.index.data(), result.value.data(), capacity,
+                         &kept));
+    result.index.resize(size_t(kept));
+    result.value.resize(size_t(kept));
+    return result;
 }
 bool cuda_propagate_integer_bounds(const Model &, std::vector<double> &, std::vector<double> &,
                                    int) {

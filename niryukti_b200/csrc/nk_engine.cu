@@ -1341,6 +1341,7 @@ Engine *create_engine(const nk_csr *Ah, const nk_csr *Qh, const double *hc, cons
 
 #include "nk_solve.cuh"
 #include "nk_batch.cuh"
+#include "nk_presolve.cuh"
 
 namespace nk {
 // Copies a caller model (C ABI) into the host representation, after the
@@ -1617,6 +1618,42 @@ nk_status nk_cuda_description(char *buffer, int length) {
                       size_t(p.totalGlobalMem / (1024 * 1024)));
     });
 }
+nk_status nk_compact_csr(const nk_csr *matrix, int64_t rows, const int64_t *kept_rows,
+                         const int64_t *column_map, int64_t output_columns, int64_t *out_ptr,
+                         int64_t *out_index, double *out_value, int64_t capacity,
+                         int64_t *out_nnz) {
+    return guard([&] {
+        if (!matrix || !out_ptr || !out_nnz || (rows > 0 && !kept_rows) ||
+            (matrix->cols > 0 && !column_map) || rows < 0 || capacity < 0 || output_columns < 0)
+            throw nk::Error(NK_ERR_INVALID, "invalid compaction arguments");
+        nk::validate_csr(matrix, matrix->rows, matrix->cols, "compaction");
+        const int64_t nnz = matrix->ptr[matrix->rows];
+        for (int64_t k = 0; k < nnz; ++k)
+            if (matrix->index[k] < 0 || matrix->index[k] >= matrix->cols)
+                throw nk::Error(NK_ERR_INVALID, "compaction column index out of range");
+        int64_t previous = -1;
+        for (int64_t r = 0; r < rows; ++r) {
+            if (kept_rows[r] <= previous || kept_rows[r] >= matrix->rows)
+                throw nk::Error(NK_ERR_INVALID, "compaction row map");
+            previous = kept_rows[r];
+        }
+        previous = -1;
+        for (int64_t j = 0; j < matrix->cols; ++j) {
+            const int64_t c = column_map[j];
+            if (c < -1 || (c >= 0 && (c <= previous || c >= output_columns)))
+                throw nk::Error(NK_ERR_INVALID, "compaction column map");
+            if (c >= 0)
+                previous = c;
+        }
+        if (capacity > 0 && (!out_index || !out_value))
+            throw nk::Error(NK_ERR_INVALID, "null compaction output");
+        if (!nk_cuda_available())
+            throw nk::Error(NK_ERR_NO_DEVICE, "no CUDA device");
+        *out_nnz = nk::compact_csr(*matrix, rows, kept_rows, column_map, out_ptr, out_index,
+                                   out_value, capacity);
+    });
+}
+
 nk_status nk_hardware_info(int *available, double *free_bytes, double *total_bytes) {
     return guard([&] {
         *available = nk_cuda_available();

@@ -81,6 +81,8 @@ def library() -> C.CDLL:
     L.nk_cuda_available.restype = C.c_int
     L.nk_cuda_description.argtypes = [C.c_char_p, C.c_int]
     L.nk_hardware_info.argtypes = [C.POINTER(C.c_int), _D, _D]
+    L.nk_compact_csr.argtypes = [C.POINTER(NkCsr), C.c_int64, _I, _I, C.c_int64, _I, _I, _D,
+                                 C.c_int64, _I]
     _lib = L
     return L
 
@@ -110,6 +112,30 @@ def cuda_description() -> str:
     buf = C.create_string_buffer(256)
     check(library().nk_cuda_description(buf, 256))
     return buf.value.decode()
+
+
+def compact_csr(ptr, idx, val, cols, kept_rows, column_map, output_columns):
+    """cuda_compact_matrix (src/cuda.cu:978-1032): the CSR of `kept_rows` with
+    the columns renumbered by `column_map` (-1 drops a column), on the GPU.
+    Returns (ptr, idx, val)."""
+    ptr = np.ascontiguousarray(ptr, dtype=np.int64)
+    idx = np.ascontiguousarray(idx, dtype=np.int64)
+    val = np.ascontiguousarray(val, dtype=np.float64)
+    kept = np.ascontiguousarray(kept_rows, dtype=np.int64)
+    cmap = np.ascontiguousarray(column_map, dtype=np.int64)
+    rows = len(ptr) - 1
+    capacity = int(np.sum(ptr[kept + 1] - ptr[kept])) if len(kept) else 0
+    out_ptr = np.zeros(len(kept) + 1, dtype=np.int64)
+    out_idx = np.zeros(max(1, capacity), dtype=np.int64)
+    out_val = np.zeros(max(1, capacity))
+    kept_nnz = C.c_int64()
+    a = NkCsr(rows, int(cols), ptr.ctypes.data_as(_I), idx.ctypes.data_as(_I), _d(val))
+    check(library().nk_compact_csr(C.byref(a), len(kept), kept.ctypes.data_as(_I),
+                                   cmap.ctypes.data_as(_I), int(output_columns),
+                                   out_ptr.ctypes.data_as(_I), out_idx.ctypes.data_as(_I),
+                                   _d(out_val), capacity, C.byref(kept_nnz)))
+    k = kept_nnz.value
+    return out_ptr, out_idx[:k].copy(), out_val[:k].copy()
 
 
 def hardware_info() -> dict:

@@ -69,6 +69,7 @@ Options make_options(const char *text) {
         else if (k == "gpu_indices") o.gpu_indices = v;
         else if (k == "matrix_precision") o.matrix_precision = v;
         else if (k == "polishing") o.polishing = v == "1";
+        else if (k == "gpu_presolve") o.gpu_presolve = v == "1";
         else throw std::runtime_error("unknown option " + k);
     }
     return o;

@@ -114,3 +114,19 @@ def test_bridged_batch_relaxations_checks_bounds(bridged):
     hi[0, 5] = model.ub[5] + 1.0
     with pytest.raises(RuntimeError, match="Invalid batch bounds"):
         bridged.model(model).batch_relaxations(lo, hi, tol=1e-6)
+
+
+@pytest.mark.parametrize("name", ["presolve", "random_11", "power_law", "large"])
+def test_bridged_gpu_presolve_compaction_bit_exact(bridged, reference, name):
+    """prepare with --gpu-presolve in the reference's own presolve: the kept
+    rows and columns are compacted by the engine (cuda_compact_matrix), and the
+    prepared model must be bit-identical to the reference's CPU prepare."""
+    from tests.test_host import MODELS, random_presolve_model, same
+    model = (random_presolve_model(21, m=30000, n=70000, per_col=6, fixed=4000, dups=2500,
+                                   redundant=1000) if name == "large" else MODELS[name]())
+    mine = bridged.model(model).prepare(presolve=True, gpu_presolve=True)
+    ref = reference.model(model).prepare(presolve=True)
+    assert ("failure" in mine) == ("failure" in ref)
+    for key in ("ptr", "idx", "val", "c", "lb", "ub", "rl", "ru", "cols", "rows", "lower_rows",
+                "upper_rows", "fixed", "column_scale", "row_scale"):
+        same(mine[key], ref[key], key)

@@ -292,3 +292,40 @@ def test_very_long_rows_and_columns_parity(gpu, oracle):
             assert g.rejected_steps() == c2.rejected_steps()
             for u, w in zip(g.candidates(), c2.candidates()):
                 near(u, w, 1e-9)
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_compact_csr_matches_host_compaction(gpu, seed):
+    """cuda_compact_matrix on the GPU against the host restriction of the same
+    CSR: kept rows in order, kept columns renumbered, entries in source order --
+    bit-identical (an integer / byte operation).  Includes empty rows, rows of
+    more than 32 entries and a dropped-everything row."""
+    rng = np.random.default_rng(seed)
+    m = synth.power_law_lp(m=3000, n=6000, nnz=60000, seed=seed, len_hi=2000)
+    kept = np.sort(rng.choice(m.m, 2000, replace=False))
+    keep_col = rng.random(m.n) < 0.7
+    cmap = np.where(keep_col, np.cumsum(keep_col) - 1, -1)
+    out_cols = int(keep_col.sum())
+    ptr, idx, val = gpu.compact_csr(m.ptr, m.idx, m.val, m.n, kept, cmap, out_cols)
+    want_ptr, want_idx, want_val = [0], [], []
+    for i in kept:
+        cols = m.idx[m.ptr[i]:m.ptr[i + 1]]
+        vals = m.val[m.ptr[i]:m.ptr[i + 1]]
+        sel = cmap[cols] >= 0
+        want_idx.extend(cmap[cols[sel]].tolist())
+        want_val.extend(vals[sel].tolist())
+        want_ptr.append(len(want_idx))
+    assert np.array_equal(ptr, want_ptr)
+    assert np.array_equal(idx, want_idx)
+    assert np.array_equal(val.view(np.int64), np.array(want_val).view(np.int64))
+
+
+def test_compact_csr_rejects_bad_maps(gpu):
+    m = synth.random_lp(m=50, n=80, per_col=3, seed=1)
+    cmap = np.arange(m.n)
+    with pytest.raises(gpu.EngineError, match="row map"):
+        gpu.compact_csr(m.ptr, m.idx, m.val, m.n, [3, 2], cmap, m.n)
+    bad = cmap.copy()
+    bad[5] = 2  # not increasing
+    with pytest.raises(gpu.EngineError, match="column map"):
+        gpu.compact_csr(m.ptr, m.idx, m.val, m.n, [0, 1], bad, m.n)
