@@ -352,6 +352,19 @@ nk_status nk_compact_csr(const nk_csr *matrix, int64_t rows, const int64_t *kept
                          int64_t *out_index, double *out_value, int64_t capacity,
                          int64_t *out_nnz);
 
+/* cuda_propagate_integer_bounds(model, lb, ub, passes) -- src/cuda.cu:448-529,
+ * 1033-1135; callers src/solver.cpp:227-240 (--gpu-presolve) and the
+ * branch-and-bound nodes (src/mip.cpp:710-720).  `passes` rounds of
+ * activity-based bound proposals over A (m x n): per row, the activity range
+ * from lb / ub with directed rounding, then for each entry the bound it
+ * implies on its column, rounded inward for integer[j] != 0 columns, kept when
+ * tighter.  lb / ub (n, host) are updated in place; *feasible = 0 when a row's
+ * activity range misses [rl, ru] or a column's bounds cross.  The results are
+ * proposals: the reference proves them again on the host before using them. */
+nk_status nk_propagate_bounds(const nk_csr *A, const int *integer, const double *rl,
+                              const double *ru, double *lb, double *ub, int passes,
+                              int *feasible);
+
 int nk_cuda_available(void);
 nk_status nk_cuda_description(char *buffer, int length);
 nk_status nk_hardware_info(int *available, double *free_bytes, double *total_bytes);

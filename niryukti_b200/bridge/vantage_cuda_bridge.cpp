@@ -12,11 +12,12 @@
 //
 // cuda_batch_relaxations (the box variants of one LP relaxation that the
 // branch-and-bound driver scores for strong branching) runs on the engine's
-// batched solver, and cuda_compact_matrix (prepare's CSR step under
-// --gpu-presolve) on its compaction kernels.  The other side entries of the
-// CUDA build, which are not part of the PDHG path (cuda_linear_solve,
-// cuda_propagate_integer_bounds), report that the B200 engine does not provide
-// them, exactly where a CPU build reports that CUDA is missing.
+// batched solver, and the two GPU presolve steps of --gpu-presolve
+// (cuda_compact_matrix, cuda_propagate_integer_bounds) on its presolve kernels.
+// The remaining side entry of the CUDA build, which is not part of the PDHG
+// path (cuda_linear_solve, the barrier's Newton solve), reports that the B200
+// engine does not provide it, exactly where a CPU build reports that CUDA is
+// missing.
 #include "internal.hpp"
 #include "nk_pdhg.h"
 
@@ -216,9 +217,28 @@ Sparse cuda_compact_matrix(const Sparse &matrix, const std::vector<int64_t> &row
     result.value.resize(size_t(kept));
     return result;
 }
-bool cuda_propagate_integer_bounds(const Model &, std::vector<double> &, std::vector<double> &,
-                                   int) {
-    throw std::runtime_error("GPU propagation is not provided by the B200 PDHG engine");
+// cuda_propagate_integer_bounds (src/cuda.cu:1033-1135): the reference's checks
+// and messages, then `passes` rounds of directed-rounding proposals on the GPU
+// (nk_propagate_bounds).  Integer and binary columns round inward.
+bool cuda_propagate_integer_bounds(const Model &m, std::vector<double> &lb,
+                                   std::vector<double> &ub, int passes) {
+    m.validate();
+    if (lb.size() != m.c.size() || ub.size() != m.c.size() || passes < 0 || passes > 100)
+        throw std::runtime_error("GPU propagation dimensions/pass limit");
+    for (size_t j = 0; j < lb.size(); ++j)
+        if (std::isnan(lb[j]) || std::isnan(ub[j]) || lb[j] < m.lb[j] || ub[j] > m.ub[j] ||
+            lb[j] > ub[j])
+            throw std::runtime_error("Invalid GPU propagation bounds");
+    if (m.A.rows == 0 || passes == 0)
+        return true;
+    std::vector<int> integer(m.c.size(), 0);
+    for (size_t j = 0; j < m.types.size() && j < integer.size(); ++j)
+        integer[j] = m.types[j] != VarType::Continuous;
+    nk_csr a{m.A.rows, m.A.cols, m.A.ptr.data(), m.A.index.data(), m.A.value.data()};
+    int feasible = 0;
+    check(nk_propagate_bounds(&a, integer.data(), m.rl.data(), m.ru.data(), lb.data(), ub.data(),
+                              passes, &feasible));
+    return feasible != 0;
 }
 // cuda_batch_relaxations (src/cuda.cu:1136-1266): the same argument checks,
 // start point (initial_x clamped into each box, initial_y), limits and result

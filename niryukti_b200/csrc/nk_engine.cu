@@ -1654,6 +1654,27 @@ nk_status nk_compact_csr(const nk_csr *matrix, int64_t rows, const int64_t *kept
     });
 }
 
+nk_status nk_propagate_bounds(const nk_csr *A, const int *integer, const double *rl,
+                              const double *ru, double *lb, double *ub, int passes,
+                              int *feasible) {
+    return guard([&] {
+        if (!A || !feasible || !rl || !ru || (A->cols > 0 && (!integer || !lb || !ub)) ||
+            passes < 0 || passes > 100)
+            throw nk::Error(NK_ERR_INVALID, "invalid propagation arguments");
+        nk::validate_csr(A, A->rows, A->cols, "propagation");
+        const int64_t nnz = A->ptr[A->rows];
+        for (int64_t k = 0; k < nnz; ++k)
+            if (A->index[k] < 0 || A->index[k] >= A->cols)
+                throw nk::Error(NK_ERR_INVALID, "propagation column index out of range");
+        for (int64_t j = 0; j < A->cols; ++j)
+            if (std::isnan(lb[j]) || std::isnan(ub[j]) || lb[j] > ub[j])
+                throw nk::Error(NK_ERR_INVALID, "invalid propagation bounds");
+        if (A->rows > 0 && passes > 0 && !nk_cuda_available())
+            throw nk::Error(NK_ERR_NO_DEVICE, "no CUDA device");
+        *feasible = nk::propagate_bounds(*A, integer, rl, ru, lb, ub, passes) ? 1 : 0;
+    });
+}
+
 nk_status nk_hardware_info(int *available, double *free_bytes, double *total_bytes) {
     return guard([&] {
         *available = nk_cuda_available();

@@ -83,6 +83,8 @@ def library() -> C.CDLL:
     L.nk_hardware_info.argtypes = [C.POINTER(C.c_int), _D, _D]
     L.nk_compact_csr.argtypes = [C.POINTER(NkCsr), C.c_int64, _I, _I, C.c_int64, _I, _I, _D,
                                  C.c_int64, _I]
+    L.nk_propagate_bounds.argtypes = [C.POINTER(NkCsr), C.POINTER(C.c_int), _D, _D, _D, _D,
+                                      C.c_int, C.POINTER(C.c_int)]
     _lib = L
     return L
 
@@ -136,6 +138,27 @@ def compact_csr(ptr, idx, val, cols, kept_rows, column_map, output_columns):
                                    _d(out_val), capacity, C.byref(kept_nnz)))
     k = kept_nnz.value
     return out_ptr, out_idx[:k].copy(), out_val[:k].copy()
+
+
+def propagate_bounds(model, integer, lb, ub, passes=5):
+    """cuda_propagate_integer_bounds (src/cuda.cu:448-529, 1033-1135) on the GPU:
+    `passes` rounds of directed-rounding bound proposals.  Returns
+    (feasible, lb, ub)."""
+    lb = np.array(lb, dtype=np.float64)
+    ub = np.array(ub, dtype=np.float64)
+    flags = np.ascontiguousarray(np.asarray(integer, dtype=np.int32))
+    ptr = np.ascontiguousarray(model.ptr, dtype=np.int64)
+    idx = np.ascontiguousarray(model.idx, dtype=np.int64)
+    val = np.ascontiguousarray(model.val, dtype=np.float64)
+    rl = np.ascontiguousarray(model.rl, dtype=np.float64)
+    ru = np.ascontiguousarray(model.ru, dtype=np.float64)
+    a = NkCsr(int(model.m), int(model.n), ptr.ctypes.data_as(_I), idx.ctypes.data_as(_I),
+              _d(val))
+    ok = C.c_int()
+    check(library().nk_propagate_bounds(C.byref(a), flags.ctypes.data_as(C.POINTER(C.c_int)),
+                                        _d(rl), _d(ru), _d(lb), _d(ub), int(passes),
+                                        C.byref(ok)))
+    return bool(ok.value), lb, ub
 
 
 def hardware_info() -> dict:

@@ -96,9 +96,27 @@ class Oracle:
         L.orc_infeasibility_bound.restype = C.c_double
         L.orc_scale.restype = C.c_void_p
         L.orc_scale.argtypes = [C.c_void_p, C.c_int, _D, _D, _D]
+        L.orc_propagate_bounds.argtypes = [C.c_int64, C.c_int64, _I, _I, _D,
+                                           C.POINTER(C.c_int), _D, _D, _D, _D, C.c_int]
         L.orc_model_get.argtypes = [C.c_void_p, _I, _I, _D, _D, _D, _D, _D, _D, _D, _D]
         L.orc_solve.argtypes = [C.c_void_p, C.c_double, C.c_int64, C.c_double, C.c_int, C.c_int,
                                 C.c_int, C.c_int, _D, _D, _D]
+
+    def propagate_bounds(self, model, integer, lb, ub, passes=5):
+        """Directed-rounding bound proposals (cuda_propagate_integer_bounds,
+        src/cuda.cu:448-529); returns (feasible, lb, ub)."""
+        lb = np.array(lb, dtype=np.float64)
+        ub = np.array(ub, dtype=np.float64)
+        flags = np.ascontiguousarray(np.asarray(integer, dtype=np.int32))
+        ptr = np.ascontiguousarray(model.ptr, dtype=np.int64)
+        idx = np.ascontiguousarray(model.idx, dtype=np.int64)
+        val = np.ascontiguousarray(model.val, dtype=np.float64)
+        rl = np.ascontiguousarray(model.rl, dtype=np.float64)
+        ru = np.ascontiguousarray(model.ru, dtype=np.float64)
+        ok = self.lib.orc_propagate_bounds(model.m, model.n, _i(ptr), _i(idx), _d(val),
+                                           flags.ctypes.data_as(C.POINTER(C.c_int)),
+                                           _d(rl), _d(ru), _d(lb), _d(ub), passes)
+        return bool(ok), lb, ub
 
     def error(self):
         return self.lib.orc_last_error().decode()

@@ -3,6 +3,7 @@
  * where the reference uses long double. */
 #define _GNU_SOURCE
 #include "pdhg_oracle.h"
+#include <fenv.h>
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -952,4 +953,117 @@ finish:
     free(cx); free(cy); free(ax_); free(ay_); free(epochx); free(epochy); free(cs); free(rs);
     orc_model_free(M);
     return 0;
+}
+
+/* ------------------------------------------------------------------ bound propagation
+ * Directed-rounding arithmetic: each operation runs under its own rounding
+ * mode (the file is compiled with -frounding-math, and results pass through
+ * volatile so the operation happens while the mode is set). */
+static double rounded(int mode, int op, double a, double b) {
+    volatile double x = a, y = b, r;
+    fesetround(mode);
+    switch (op) {
+    case 0: r = x + y; break;
+    case 1: r = x - y; break;
+    case 2: r = x * y; break;
+    default: r = x / y; break;
+    }
+    fesetround(FE_TONEAREST);
+    return r;
+}
+#define ADD_DN(a, b) rounded(FE_DOWNWARD, 0, a, b)
+#define ADD_UP(a, b) rounded(FE_UPWARD, 0, a, b)
+#define SUB_DN(a, b) rounded(FE_DOWNWARD, 1, a, b)
+#define SUB_UP(a, b) rounded(FE_UPWARD, 1, a, b)
+#define MUL_DN(a, b) rounded(FE_DOWNWARD, 2, a, b)
+#define MUL_UP(a, b) rounded(FE_UPWARD, 2, a, b)
+#define DIV_DN(a, b) rounded(FE_DOWNWARD, 3, a, b)
+#define DIV_UP(a, b) rounded(FE_UPWARD, 3, a, b)
+
+/* propagate_rows and the pass loop of cuda_propagate_integer_bounds
+ * (src/cuda.cu:468-529, 1110-1134): proposals of a pass read the bounds of the
+ * previous pass; the tightest proposal per column wins. */
+int orc_propagate_bounds(int64_t m, int64_t n, const int64_t *ptr, const int64_t *idx,
+                         const double *val, const int *integer, const double *rl, const double *ru,
+                         double *lb, double *ub, int passes) {
+    if (m == 0 || passes == 0)
+        return 1;
+    double *olb = malloc(sizeof(double) * (size_t)(n ? n : 1));
+    double *oub = malloc(sizeof(double) * (size_t)(n ? n : 1));
+    int failed = 0;
+    for (int pass = 0; pass < passes; ++pass) {
+        memcpy(olb, lb, sizeof(double) * (size_t)n);
+        memcpy(oub, ub, sizeof(double) * (size_t)n);
+        for (int64_t row = 0; row < m; ++row) {
+            double low = 0, high = 0;
+            int low_inf = 0, high_inf = 0;
+            for (int64_t k = ptr[row]; k < ptr[row + 1]; ++k) {
+                double v = val[k];
+                if (v == 0)
+                    continue;
+                int64_t j = idx[k];
+                double lo = MUL_DN(v, v > 0 ? olb[j] : oub[j]);
+                double hi = MUL_UP(v, v > 0 ? oub[j] : olb[j]);
+                if (isinf(lo))
+                    ++low_inf;
+                else
+                    low = ADD_DN(low, lo);
+                if (isinf(hi))
+                    ++high_inf;
+                else
+                    high = ADD_UP(high, hi);
+            }
+            if ((!low_inf && low > ru[row]) || (!high_inf && high < rl[row]))
+                failed = 1;
+            for (int64_t k = ptr[row]; k < ptr[row + 1]; ++k) {
+                double v = val[k];
+                if (v == 0)
+                    continue;
+                int64_t j = idx[k];
+                double end_low = v > 0 ? olb[j] : oub[j], end_high = v > 0 ? oub[j] : olb[j];
+                double term_low = MUL_DN(v, end_low), term_high = MUL_UP(v, end_high);
+                int tl = isinf(term_low) ? 1 : 0, th = isinf(term_high) ? 1 : 0;
+                double rest_low = (low_inf - tl) ? -INFINITY
+                                  : tl           ? low
+                                                 : SUB_DN(low, MUL_UP(v, end_low));
+                double rest_high = (high_inf - th) ? INFINITY
+                                   : th            ? high
+                                                   : SUB_UP(high, MUL_DN(v, end_high));
+                double l = -INFINITY, u = INFINITY;
+                if (isfinite(rl[row]) && isfinite(rest_high)) {
+                    double num = SUB_DN(rl[row], rest_high);
+                    if (v > 0)
+                        l = DIV_DN(num, v);
+                    else
+                        u = DIV_UP(num, v);
+                }
+                if (isfinite(ru[row]) && isfinite(rest_low)) {
+                    double num = SUB_UP(ru[row], rest_low);
+                    if (v > 0)
+                        u = DIV_UP(num, v);
+                    else
+                        l = DIV_DN(num, v);
+                }
+                int whole = integer[j] != 0;
+                if (isfinite(l) && (!whole || fabs(l) < 4503599627370496.0)) {
+                    double t = whole ? ceil(l) : l;
+                    if (t > lb[j])
+                        lb[j] = t;
+                }
+                if (isfinite(u) && (!whole || fabs(u) < 4503599627370496.0)) {
+                    double t = whole ? floor(u) : u;
+                    if (t < ub[j])
+                        ub[j] = t;
+                }
+            }
+        }
+    }
+    free(olb);
+    free(oub);
+    if (failed)
+        return 0;
+    for (int64_t j = 0; j < n; ++j)
+        if (lb[j] > ub[j])
+            return 0;
+    return 1;
 }

@@ -72,6 +72,15 @@ int orc_solve(const orc_model *, double tol, int64_t iteration_limit, double tim
               int check_every, int scaling_passes, int adaptive, int restart, double *x_out,
               double *y_out, double *stats);
 
+/* Activity-based bound proposals with directed rounding, `passes` rounds over
+ * A (m x n) -- the algorithm of cuda_propagate_integer_bounds
+ * (src/cuda.cu:448-529, 1033-1135), restated sequentially with the rounding
+ * mode switched per operation.  lb / ub are updated in place; returns 1 when
+ * feasible, 0 when a row's activity range misses [rl, ru] or bounds cross. */
+int orc_propagate_bounds(int64_t m, int64_t n, const int64_t *ptr, const int64_t *idx,
+                         const double *val, const int *integer, const double *rl, const double *ru,
+                         double *lb, double *ub, int passes);
+
 /* accessors for a model's arrays (used to read orc_scale results) */
 void orc_model_get(const orc_model *, int64_t *ptr, int64_t *idx, double *val, double *c,
                    double *q, double *lb, double *ub, double *rl, double *ru, double *offset);

@@ -130,3 +130,18 @@ def test_bridged_gpu_presolve_compaction_bit_exact(bridged, reference, name):
     for key in ("ptr", "idx", "val", "c", "lb", "ub", "rl", "ru", "cols", "rows", "lower_rows",
                 "upper_rows", "fixed", "column_scale", "row_scale"):
         same(mine[key], ref[key], key)
+
+
+def test_bridged_solve_with_gpu_presolve(bridged, reference):
+    """The reference's solve with --gpu-presolve through the bridge: bound
+    proposals (cuda_propagate_integer_bounds) proven again by the reference's
+    host code, CSR compaction (cuda_compact_matrix), then the engine's PDHG --
+    the answer of the plain CPU solve."""
+    from tests.conftest import load_golden
+    model, d = load_golden("solve_small_lp")
+    want = json.loads(str(d["result"]))
+    r = bridged.model(model).solve(method="pdhg", device="cuda", gpu_presolve=True,
+                                   iteration_limit=200000)
+    assert r["status"] == want["status"] == "OPTIMAL"
+    assert r["kkt"] <= 1e-6
+    assert abs(r["objective"] - want["objective"]) <= 2e-6 * (1 + abs(want["objective"]))

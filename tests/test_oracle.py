@@ -240,3 +240,31 @@ def test_reference_cpu_build_has_no_batched_relaxations(reference):
     model = synth.random_lp(m=50, n=120, per_col=3, seed=2)
     with pytest.raises(RuntimeError, match="require a CUDA build"):
         reference.model(model).batch_relaxations(model.lb[None, :], model.ub[None, :], tol=1e-6)
+
+
+def _one_row(vals, lb, ub, rl, ru):
+    n = len(vals)
+    return synth.Model(m=1, n=n, ptr=np.array([0, n]), idx=np.arange(n), val=np.array(vals, float),
+                       c=np.zeros(n), q=np.zeros(n), lb=np.array(lb, float),
+                       ub=np.array(ub, float), rl=np.array([rl], float), ru=np.array([ru], float))
+
+
+def test_oracle_propagation_known_answers(oracle):
+    """Bound proposals of cuda_propagate_integer_bounds (src/cuda.cu:468-529) on
+    one-row cases: integer columns round inward, continuous ones keep the
+    directed-rounded bound, a row whose activity range misses its bounds is
+    infeasible."""
+    m = _one_row([1, 1], [0, 0], [10, 10], -np.inf, 1.5)
+    assert oracle.propagate_bounds(m, [1, 1], m.lb, m.ub)[2].tolist() == [1.0, 1.0]
+    assert oracle.propagate_bounds(m, [0, 0], m.lb, m.ub)[2].tolist() == [1.5, 1.5]
+    m = _one_row([1, 1], [1, 1], [10, 10], -np.inf, 1.5)
+    assert oracle.propagate_bounds(m, [0, 0], m.lb, m.ub)[0] is False
+    # 3 x = 1: the bounds bracket 1/3 by adjacent doubles (round down / round up)
+    m = _one_row([3], [0], [10], 1, 1)
+    ok, lb, ub = oracle.propagate_bounds(m, [0], m.lb, m.ub)
+    assert ok and lb[0] <= 1 / 3 <= ub[0] and np.nextafter(lb[0], 1) == ub[0]
+    # 0 <= x0 - x1 <= 2 with x0 in [0, 5] and x1 free bounds x1 to [-2, 5]; x0
+    # gains nothing, since the free x1 leaves the rest of its row unbounded
+    m = _one_row([1, -1], [0, -np.inf], [5, np.inf], 0, 2)
+    ok, lb, ub = oracle.propagate_bounds(m, [0, 0], m.lb, m.ub)
+    assert ok and lb.tolist() == [0.0, -2.0] and ub.tolist() == [5.0, 5.0]
