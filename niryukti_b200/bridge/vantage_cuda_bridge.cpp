@@ -12,12 +12,9 @@
 //
 // cuda_batch_relaxations (the box variants of one LP relaxation that the
 // branch-and-bound driver scores for strong branching) runs on the engine's
-// batched solver, and the two GPU presolve steps of --gpu-presolve
-// (cuda_compact_matrix, cuda_propagate_integer_bounds) on its presolve kernels.
-// The remaining side entry of the CUDA build, which is not part of the PDHG
-// path (cuda_linear_solve, the barrier's Newton solve), reports that the B200
-// engine does not provide it, exactly where a CPU build reports that CUDA is
-// missing.
+// batched solver, the two GPU presolve steps of --gpu-presolve
+// (cuda_compact_matrix, cuda_propagate_integer_bounds) on its presolve kernels,
+// and the barrier method's Newton solve (cuda_linear_solve) on its BiCGSTAB.
 #include "internal.hpp"
 #include "nk_pdhg.h"
 
@@ -353,9 +350,36 @@ std::vector<Result> cuda_batch_relaxations(const Model &m,
         r.seconds = elapsed();
     return results;
 }
-std::vector<double> cuda_linear_solve(const Sparse &, const std::vector<double> &,
-                                      const Options &, bool, double) {
-    throw std::runtime_error("GPU Newton solve is not provided by the B200 PDHG engine");
+// cuda_linear_solve (src/cuda.cu:1328-1434): the barrier's Newton systems on the
+// engine's device-resident BiCGSTAB (nk_linear_solve), then the reference's own
+// acceptance test of the solution (finite, max-norm residual within tolerance).
+std::vector<double> cuda_linear_solve(const Sparse &matrix, const std::vector<double> &rhs,
+                                      const Options &o, bool fp32_matrix, double tolerance) {
+    if (matrix.rows != matrix.cols || rhs.size() != size_t(matrix.rows))
+        throw std::runtime_error("Newton matrix dimensions");
+    const size_t n = rhs.size();
+    if (!n)
+        return {};
+    if (stop_requested(o))
+        throw std::runtime_error("GPU Newton solve interrupted or time-limited");
+    nk_csr a{matrix.rows, matrix.cols, matrix.ptr.data(), matrix.index.data(), matrix.value.data()};
+    std::vector<double> solution(n);
+    int converged = 0, timed_out = 0;
+    check(nk_linear_solve(&a, rhs.data(), fp32_matrix ? 1 : 0, std::max(0., o.time_limit),
+                          solution.data(), &converged, &timed_out));
+    if (timed_out)
+        throw std::runtime_error("GPU Newton solve interrupted or time-limited");
+    auto activity = matrix.multiply(solution);
+    long double error = 0, rhsnorm = 0;
+    for (size_t j = 0; j < n; ++j) {
+        if (!std::isfinite(solution[j]))
+            throw std::runtime_error("Nonfinite GPU Newton solution");
+        error = std::max(error, std::abs((long double)activity[j] - rhs[j]));
+        rhsnorm = std::max(rhsnorm, std::abs((long double)rhs[j]));
+    }
+    if (!converged || error > (long double)tolerance * (1 + rhsnorm))
+        throw std::runtime_error("GPU Newton residual/breakdown check failed");
+    return solution;
 }
 
 } // namespace vantage

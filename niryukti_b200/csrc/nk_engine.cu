@@ -1342,6 +1342,7 @@ Engine *create_engine(const nk_csr *Ah, const nk_csr *Qh, const double *hc, cons
 #include "nk_solve.cuh"
 #include "nk_batch.cuh"
 #include "nk_presolve.cuh"
+#include "nk_newton.cuh"
 
 namespace nk {
 // Copies a caller model (C ABI) into the host representation, after the
@@ -1672,6 +1673,29 @@ nk_status nk_propagate_bounds(const nk_csr *A, const int *integer, const double 
         if (A->rows > 0 && passes > 0 && !nk_cuda_available())
             throw nk::Error(NK_ERR_NO_DEVICE, "no CUDA device");
         *feasible = nk::propagate_bounds(*A, integer, rl, ru, lb, ub, passes) ? 1 : 0;
+    });
+}
+
+nk_status nk_linear_solve(const nk_csr *K, const double *rhs, int fp32_matrix, double time_limit,
+                          double *x, int *converged, int *timed_out) {
+    return guard([&] {
+        if (!K || !converged || !timed_out || K->rows != K->cols || K->rows < 0 ||
+            (K->rows > 0 && (!rhs || !x)) || !(time_limit >= 0))
+            throw nk::Error(NK_ERR_INVALID, "Newton matrix dimensions");
+        nk::validate_csr(K, K->rows, K->cols, "Newton");
+        const int64_t nnz = K->ptr[K->rows];
+        for (int64_t k = 0; k < nnz; ++k)
+            if (K->index[k] < 0 || K->index[k] >= K->cols)
+                throw nk::Error(NK_ERR_INVALID, "Newton column index out of range");
+        *converged = 1;
+        *timed_out = 0;
+        if (K->rows == 0)
+            return;
+        if (!nk_cuda_available())
+            throw nk::Error(NK_ERR_NO_DEVICE, "no CUDA device");
+        bool late = false;
+        *converged = nk::newton_solve(*K, rhs, fp32_matrix != 0, time_limit, x, &late) ? 1 : 0;
+        *timed_out = late ? 1 : 0;
     });
 }
 

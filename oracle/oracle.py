@@ -312,6 +312,19 @@ class Reference:
         L.ref_cuda_available.restype = C.c_int
         L.ref_batch_relaxations.argtypes = [C.c_void_p, C.c_int, _D, _D, _D, _D, C.c_char_p, _D,
                                             C.POINTER(C.c_int), _D, _D]
+        L.ref_linear_solve.argtypes = [C.c_int64, _I, _I, _D, _D, C.c_int, C.c_double, _D]
+
+    def linear_solve(self, ptr, idx, val, rhs, fp32_matrix=False, tolerance=1e-7):
+        """cuda_linear_solve(K, rhs, Options(), fp32_matrix, tolerance)."""
+        ptr = np.ascontiguousarray(ptr, dtype=np.int64)
+        idx = np.ascontiguousarray(idx, dtype=np.int64)
+        val = np.ascontiguousarray(val, dtype=np.float64)
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        x = np.zeros(len(ptr) - 1)
+        if self.lib.ref_linear_solve(len(ptr) - 1, _i(ptr), _i(idx), _d(val), _d(rhs),
+                                     int(bool(fp32_matrix)), float(tolerance), _d(x)) != 0:
+            raise RuntimeError(self.error())
+        return x
 
     def error(self):
         return self.lib.ref_last_error().decode()
@@ -378,6 +391,7 @@ class RefModel:
                            "removed_rows")
         r = dict(zip(keys, st.tolist()))
         r["status"] = status.value.decode()
+        r["message"] = self.r.error()
         r["x"], r["y"] = x, y
         return r
 

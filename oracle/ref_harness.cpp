@@ -198,6 +198,7 @@ int ref_solve(ref_model *r, const char *opts, double *x_out, double *y_out, doub
         if (y_out && res.y.size() == r->m.rl.size())
             std::memcpy(y_out, res.y.data(), res.y.size() * sizeof(double));
         std::snprintf(status, size_t(status_len), "%s", res.status.c_str());
+        set_error(res.message.c_str()); // the result's message (empty on success)
         return 0;
     } catch (const std::exception &e) {
         set_error(e.what());
@@ -373,6 +374,27 @@ void ref_prepared_get(ref_prepared *h, int64_t *ptr, int64_t *idx, double *val, 
     cp(qval, m.Q.value);
 }
 int ref_cuda_available(void) { return cuda_available() ? 1 : 0; }
+
+// cuda_linear_solve(matrix, rhs, options, fp32_matrix, tolerance) --
+// src/internal.hpp:49-50: K (n x n CSR) x = rhs; x_out gets the solution.
+int ref_linear_solve(int64_t n, const int64_t *ptr, const int64_t *idx, const double *val,
+                     const double *rhs, int fp32_matrix, double tolerance, double *x_out) {
+    try {
+        Sparse k;
+        k.rows = k.cols = n;
+        k.ptr.assign(ptr, ptr + n + 1);
+        k.index.assign(idx, idx + ptr[n]);
+        k.value.assign(val, val + ptr[n]);
+        Options o;
+        auto x = cuda_linear_solve(k, std::vector<double>(rhs, rhs + n), o, fp32_matrix != 0,
+                                   tolerance);
+        std::memcpy(x_out, x.data(), x.size() * sizeof(double));
+        return 0;
+    } catch (const std::exception &e) {
+        set_error(e.what());
+        return -1;
+    }
+}
 
 // cuda_batch_relaxations(model, lower, upper, options) -- src/internal.hpp:60-62.
 // lower / upper: `boxes` rows of n bounds; x0 / y0 (may be NULL) become

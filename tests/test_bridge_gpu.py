@@ -145,3 +145,14 @@ def test_bridged_solve_with_gpu_presolve(bridged, reference):
     assert r["status"] == want["status"] == "OPTIMAL"
     assert r["kkt"] <= 1e-6
     assert abs(r["objective"] - want["objective"]) <= 2e-6 * (1 + abs(want["objective"]))
+
+
+def test_bridged_linear_solve(bridged):
+    """cuda_linear_solve through the bridge (the barrier's Newton solve): the
+    engine's BiCGSTAB, then the reference's acceptance test of the solution
+    (finite, max-norm residual within the tolerance), on a nonsymmetric,
+    diagonally dominant system."""
+    from tests.test_engine_gpu import _newton_system
+    ptr, idx, val, dense, rhs = _newton_system(2000)
+    x = bridged.linear_solve(ptr, idx, val, rhs, tolerance=1e-7)
+    assert np.max(np.abs(dense @ x - rhs)) <= 1e-7 * (1 + np.max(np.abs(rhs)))

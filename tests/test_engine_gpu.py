@@ -367,3 +367,33 @@ def test_propagate_bounds_detects_infeasible_row(gpu, oracle):
     m.rl[7] = 1e9  # no point in the box reaches it
     ok_g = gpu.propagate_bounds(m, integer, lb, ub, 3)[0]
     assert ok_g is False and oracle.propagate_bounds(m, integer, lb, ub, 3)[0] is False
+
+
+def _newton_system(n, seed=11):
+    """A nonsymmetric, diagonally dominant sparse system (CSR and dense)."""
+    rng = np.random.default_rng(seed)
+    rows = np.repeat(np.arange(n), 6)
+    cols = rng.integers(0, n, rows.size)
+    vals = rng.standard_normal(rows.size)
+    dense = np.zeros((n, n))
+    np.add.at(dense, (rows, cols), vals)
+    dense[np.arange(n), np.arange(n)] += 8 + np.abs(dense).sum(1)
+    nz = dense != 0
+    ptr = np.concatenate([[0], np.cumsum(nz.sum(1))]).astype(np.int64)
+    idx = np.nonzero(nz)[1].astype(np.int64)
+    return ptr, idx, dense[nz], dense, rng.standard_normal(n)
+
+
+@pytest.mark.parametrize("fp32", [False, True])
+def test_linear_solve_bicgstab(gpu, fp32):
+    """cuda_linear_solve's BiCGSTAB on a nonsymmetric, diagonally dominant sparse
+    system: converged, and the solution within the target the reference sets
+    (1e-10 relative residual in FP64, 1e-6 with FP32 values) of the dense solve."""
+    ptr, idx, val, dense, rhs = _newton_system(3000)
+    x, ok = gpu.linear_solve(ptr, idx, val, rhs, fp32_matrix=fp32)
+    assert ok
+    want = np.linalg.solve(dense, rhs)
+    tol = 1e-5 if fp32 else 1e-9
+    assert np.max(np.abs(x - want)) <= tol * (1 + np.max(np.abs(want)))
+    if not fp32:
+        assert np.linalg.norm(dense @ x - rhs) <= 1e-10 * (1 + np.linalg.norm(rhs)) * 10
