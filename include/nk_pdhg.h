@@ -370,12 +370,15 @@ nk_status nk_propagate_bounds(const nk_csr *A, const int *integer, const double 
  * (src/barrier.cpp:280-300).  BiCGSTAB for K x = rhs (K: n x n CSR, host
  * arrays; FP32 values with FP64 vectors and sums when fp32_matrix), from x = 0,
  * to the residual target (fp32 ? 1e-6 : 1e-10) (1 + |rhs|), at most
- * min(20000, 10 n + 100) iterations.  x (n) receives the last iterate;
- * *converged = 1 when the target was met, *timed_out = 1 when time_limit
- * seconds ran out first.  The caller checks the residual of x, as the
- * reference does, before using it. */
-nk_status nk_linear_solve(const nk_csr *K, const double *rhs, int fp32_matrix, double time_limit,
-                          double *x, int *converged, int *timed_out);
+ * min(20000, 10 n + 100) iterations.  precondition = 0 runs the reference's
+ * iteration exactly; 1 adds a diagonal right preconditioner (|K_ii|, or the
+ * row's Schur-complement diagonal where a saddle point's regularised block
+ * leaves K_ii near zero), which the barrier's badly scaled Newton matrices
+ * need.  x (n) receives the last iterate; *converged = 1 when the target was
+ * met, *timed_out = 1 when time_limit seconds ran out first.  The caller checks
+ * the residual of x, as the reference does, before using it. */
+nk_status nk_linear_solve(const nk_csr *K, const double *rhs, int fp32_matrix, int precondition,
+                          double time_limit, double *x, int *converged, int *timed_out);
 
 int nk_cuda_available(void);
 nk_status nk_cuda_description(char *buffer, int length);

@@ -351,7 +351,9 @@ std::vector<Result> cuda_batch_relaxations(const Model &m,
     return results;
 }
 // cuda_linear_solve (src/cuda.cu:1328-1434): the barrier's Newton systems on the
-// engine's device-resident BiCGSTAB (nk_linear_solve), then the reference's own
+// engine's device-resident BiCGSTAB (nk_linear_solve), diagonally right-
+// preconditioned -- the barrier's Newton matrices scale their rows over many
+// decades as the iterates approach the boundary -- then the reference's own
 // acceptance test of the solution (finite, max-norm residual within tolerance).
 std::vector<double> cuda_linear_solve(const Sparse &matrix, const std::vector<double> &rhs,
                                       const Options &o, bool fp32_matrix, double tolerance) {
@@ -365,7 +367,7 @@ std::vector<double> cuda_linear_solve(const Sparse &matrix, const std::vector<do
     nk_csr a{matrix.rows, matrix.cols, matrix.ptr.data(), matrix.index.data(), matrix.value.data()};
     std::vector<double> solution(n);
     int converged = 0, timed_out = 0;
-    check(nk_linear_solve(&a, rhs.data(), fp32_matrix ? 1 : 0, std::max(0., o.time_limit),
+    check(nk_linear_solve(&a, rhs.data(), fp32_matrix ? 1 : 0, 1, std::max(0., o.time_limit),
                           solution.data(), &converged, &timed_out));
     if (timed_out)
         throw std::runtime_error("GPU Newton solve interrupted or time-limited");

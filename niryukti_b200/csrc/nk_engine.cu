@@ -1676,8 +1676,8 @@ nk_status nk_propagate_bounds(const nk_csr *A, const int *integer, const double 
     });
 }
 
-nk_status nk_linear_solve(const nk_csr *K, const double *rhs, int fp32_matrix, double time_limit,
-                          double *x, int *converged, int *timed_out) {
+nk_status nk_linear_solve(const nk_csr *K, const double *rhs, int fp32_matrix, int precondition,
+                          double time_limit, double *x, int *converged, int *timed_out) {
     return guard([&] {
         if (!K || !converged || !timed_out || K->rows != K->cols || K->rows < 0 ||
             (K->rows > 0 && (!rhs || !x)) || !(time_limit >= 0))
@@ -1694,7 +1694,8 @@ nk_status nk_linear_solve(const nk_csr *K, const double *rhs, int fp32_matrix, d
         if (!nk_cuda_available())
             throw nk::Error(NK_ERR_NO_DEVICE, "no CUDA device");
         bool late = false;
-        *converged = nk::newton_solve(*K, rhs, fp32_matrix != 0, time_limit, x, &late) ? 1 : 0;
+        *converged = nk::newton_solve(*K, rhs, fp32_matrix != 0, precondition != 0, time_limit, x,
+                                      &late) ? 1 : 0;
         *timed_out = late ? 1 : 0;
     });
 }

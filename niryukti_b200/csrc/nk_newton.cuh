@@ -140,17 +140,64 @@ __global__ void newton_combine(int64_t n, double *out, const double *a, const do
     for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < n; j += stride)
         out[j] = ca * a[j] + cb * b[j] + cc * c[j];
 }
+// out = dinv * in (the right preconditioner), while the iteration runs
+__global__ void newton_scale(int64_t n, double *__restrict__ out, const double *__restrict__ dinv,
+                             const double *__restrict__ in, const NewtonState *st) {
+    if (st->stop)
+        return;
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < n; j += stride)
+        out[j] = dinv[j] * in[j];
+}
 __global__ void newton_mark_done(NewtonState *st) {
     if (st->stop == 3)
         st->stop = 1;
 }
 
-// Solves K x = rhs (K: n x n CSR, host arrays).  Returns true when a residual
-// met the target ((fp32 ? 1e-6 : 1e-10) (1 + |rhs|)) before breakdown, the
-// iteration cap (min(20000, 10 n + 100)) or the time limit; x gets the last
-// iterate either way.  The arguments are checked by the caller.
-inline bool newton_solve(const nk_csr &K, const double *rhs, bool fp32, double time_limit,
-                         double *x_out, bool *timed_out) {
+// Diagonal right preconditioner of a Newton matrix, 1 / (its scale) per row:
+// |K_ii| where the diagonal carries the row; where it does not (a saddle
+// point's regularised zero block, |K_ii| < 1e-8 max_j |K_ij|), the diagonal of
+// the row's Schur complement, sum_j K_ij^2 / |K_jj| over the other entries.
+// Rows with neither keep 1.
+inline std::vector<double> newton_diagonal(const nk_csr &K) {
+    const int64_t n = K.rows;
+    std::vector<double> diag(static_cast<size_t>(n), 0.0), big(static_cast<size_t>(n), 0.0),
+        dinv(static_cast<size_t>(n), 1.0);
+    for (int64_t i = 0; i < n; ++i)
+        for (int64_t k = K.ptr[i]; k < K.ptr[i + 1]; ++k) {
+            big[size_t(i)] = std::max(big[size_t(i)], std::fabs(K.value[k]));
+            if (K.index[k] == i)
+                diag[size_t(i)] += K.value[k];
+        }
+    auto carries = [&](int64_t i) {
+        return std::fabs(diag[size_t(i)]) >= 1e-8 * big[size_t(i)] && diag[size_t(i)] != 0;
+    };
+    for (int64_t i = 0; i < n; ++i) {
+        if (carries(i)) {
+            dinv[size_t(i)] = 1 / std::fabs(diag[size_t(i)]);
+            continue;
+        }
+        double schur = 0;
+        for (int64_t k = K.ptr[i]; k < K.ptr[i + 1]; ++k) {
+            const int64_t j = K.index[k];
+            if (j != i && carries(j))
+                schur += K.value[k] * K.value[k] / std::fabs(diag[size_t(j)]);
+        }
+        if (schur > 0 && std::isfinite(schur))
+            dinv[size_t(i)] = 1 / schur;
+    }
+    return dinv;
+}
+
+// Solves K x = rhs (K: n x n CSR, host arrays) by BiCGSTAB, right-preconditioned
+// by newton_diagonal when `precondition` (without it, the iteration is the
+// reference's one exactly: every scaling is by 1).  The residual r stays the
+// unpreconditioned one, so the stopping test is the reference's.  Returns true
+// when a residual met the target ((fp32 ? 1e-6 : 1e-10) (1 + |rhs|)) before
+// breakdown, the iteration cap (min(20000, 10 n + 100)) or the time limit; x
+// gets the last iterate either way.  The arguments are checked by the caller.
+inline bool newton_solve(const nk_csr &K, const double *rhs, bool fp32, bool precondition,
+                         double time_limit, double *x_out, bool *timed_out) {
     const int64_t n = K.rows, nnz = K.ptr[K.rows];
     *timed_out = false;
     cudaStream_t s = nullptr;
@@ -166,7 +213,7 @@ inline bool newton_solve(const nk_csr &K, const double *rhs, bool fp32, double t
     DevBuf<int64_t> dptr(nn + 1), didx(nz);
     DevBuf<double> val64(fp32 ? 1 : nz);
     DevBuf<float> val32(fp32 ? nz : 1);
-    DevBuf<double> x(nn), r(nn), anchor(nn), p(nn), v(nn), sv(nn), t(nn);
+    DevBuf<double> x(nn), r(nn), anchor(nn), p(nn), v(nn), sv(nn), t(nn), y(nn), z(nn), dinv(nn);
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -189,6 +236,10 @@ inline bool newton_solve(const nk_csr &K, const double *rhs, bool fp32, double t
             cuda_check(cudaMemcpyAsync(val64.p, K.value, size_t(nnz) * 8, cudaMemcpyHostToDevice, s),
                        "Newton values");
     }
+    const std::vector<double> hdinv =
+        precondition ? newton_diagonal(K) : std::vector<double>(nn, 1.0);
+    cuda_check(cudaMemcpyAsync(dinv.p, hdinv.data(), nn * 8, cudaMemcpyHostToDevice, s),
+               "Newton preconditioner");
     cuda_check(cudaMemcpyAsync(r.p, rhs, nn * 8, cudaMemcpyHostToDevice, s), "Newton rhs");
     cuda_check(cudaMemcpyAsync(anchor.p, rhs, nn * 8, cudaMemcpyHostToDevice, s), "Newton rhs");
     for (double *z : {x.p, p.p, v.p})
@@ -230,19 +281,21 @@ inline bool newton_solve(const nk_csr &K, const double *rhs, bool fp32, double t
         dot(anchor.p, r.p, &d->rho);
         newton_scalars<<<1, 1, 0, s>>>(d, 0);
         combine(p.p, r.p, p.p, v.p, 0);
-        multiply(p.p, v.p);
+        newton_scale<<<vgrid, kThreads, 0, s>>>(n, y.p, dinv.p, p.p, d); // y = M^-1 p
+        multiply(y.p, v.p);
         dot(anchor.p, v.p, &d->divisor);
         newton_scalars<<<1, 1, 0, s>>>(d, 1);
         combine(sv.p, r.p, v.p, v.p, 1);
         dot(sv.p, sv.p, &d->ss);
         newton_scalars<<<1, 1, 0, s>>>(d, 2);
-        combine(x.p, x.p, p.p, p.p, 2);
+        combine(x.p, x.p, y.p, y.p, 2);
         newton_mark_done<<<1, 1, 0, s>>>(d);
-        multiply(sv.p, t.p);
+        newton_scale<<<vgrid, kThreads, 0, s>>>(n, z.p, dinv.p, sv.p, d); // z = M^-1 s
+        multiply(z.p, t.p);
         dot(t.p, t.p, &d->tt);
         dot(t.p, sv.p, &d->ts);
         newton_scalars<<<1, 1, 0, s>>>(d, 3);
-        combine(x.p, x.p, p.p, sv.p, 3);
+        combine(x.p, x.p, y.p, z.p, 3);
         combine(r.p, sv.p, t.p, t.p, 4);
         dot(r.p, r.p, &d->rr);
         newton_scalars<<<1, 1, 0, s>>>(d, 4);

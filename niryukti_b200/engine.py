@@ -85,7 +85,7 @@ def library() -> C.CDLL:
                                  C.c_int64, _I]
     L.nk_propagate_bounds.argtypes = [C.POINTER(NkCsr), C.POINTER(C.c_int), _D, _D, _D, _D,
                                       C.c_int, C.POINTER(C.c_int)]
-    L.nk_linear_solve.argtypes = [C.POINTER(NkCsr), _D, C.c_int, C.c_double, _D,
+    L.nk_linear_solve.argtypes = [C.POINTER(NkCsr), _D, C.c_int, C.c_int, C.c_double, _D,
                                   C.POINTER(C.c_int), C.POINTER(C.c_int)]
     _lib = L
     return L
@@ -163,9 +163,10 @@ def propagate_bounds(model, integer, lb, ub, passes=5):
     return bool(ok.value), lb, ub
 
 
-def linear_solve(ptr, idx, val, rhs, fp32_matrix=False, time_limit=60.0):
+def linear_solve(ptr, idx, val, rhs, fp32_matrix=False, precondition=True, time_limit=60.0):
     """cuda_linear_solve (src/cuda.cu:1328-1434): BiCGSTAB for K x = rhs on the
-    GPU.  Returns (x, converged)."""
+    GPU (diagonally right-preconditioned unless precondition=False, which runs
+    the reference's iteration exactly).  Returns (x, converged)."""
     ptr = np.ascontiguousarray(ptr, dtype=np.int64)
     idx = np.ascontiguousarray(idx, dtype=np.int64)
     val = np.ascontiguousarray(val, dtype=np.float64)
@@ -174,8 +175,9 @@ def linear_solve(ptr, idx, val, rhs, fp32_matrix=False, time_limit=60.0):
     x = np.zeros(n)
     ok, late = C.c_int(), C.c_int()
     a = NkCsr(n, n, ptr.ctypes.data_as(_I), idx.ctypes.data_as(_I), _d(val))
-    check(library().nk_linear_solve(C.byref(a), _d(rhs), int(bool(fp32_matrix)), float(time_limit),
-                                    _d(x), C.byref(ok), C.byref(late)))
+    check(library().nk_linear_solve(C.byref(a), _d(rhs), int(bool(fp32_matrix)),
+                                    int(bool(precondition)), float(time_limit), _d(x),
+                                    C.byref(ok), C.byref(late)))
     if late.value:
         raise EngineError(3, "GPU Newton solve time-limited")
     return x, bool(ok.value)
