@@ -79,3 +79,34 @@ def test_missing_device_is_a_status():
     assert e.value.status == "NO_DEVICE"
     assert engine.hardware_info()["gpu_available"] is False
     assert engine.cuda_description() == "No CUDA device"
+
+
+def test_side_entries_check_their_arguments_before_device_use():
+    """The presolve and Newton entries refuse bad maps, bounds and shapes with a
+    status before any device call (so these run without a GPU)."""
+    m = _bad_model()
+    cmap = np.arange(m.n)
+    with pytest.raises(engine.EngineError, match="compaction row map"):
+        engine.compact_csr(m.ptr, m.idx, m.val, m.n, [4, 4], cmap, m.n)
+    with pytest.raises(engine.EngineError, match="compaction column map"):
+        engine.compact_csr(m.ptr, m.idx, m.val, m.n, [0], cmap, m.n - 1)  # map beyond the output
+    bad_lb = m.lb.copy()
+    bad_lb[3] = m.ub[3] + 1  # crossed bounds
+    with pytest.raises(engine.EngineError, match="invalid propagation bounds"):
+        engine.propagate_bounds(m, np.zeros(m.n, dtype=np.int32), bad_lb, m.ub)
+    with pytest.raises(engine.EngineError, match="invalid propagation arguments"):
+        engine.propagate_bounds(m, np.zeros(m.n, dtype=np.int32), m.lb, m.ub, passes=101)
+    rect = np.array([0, 1, 2]), np.array([0, 5]), np.array([1.0, 2.0])
+    with pytest.raises(engine.EngineError, match="Newton column index out of range"):
+        engine.linear_solve(*rect, np.ones(2))
+
+
+@pytest.mark.skipif(engine.cuda_available(), reason="checks the no-device path")
+def test_side_entries_report_a_missing_device():
+    m = _bad_model()
+    with pytest.raises(engine.EngineError) as e:
+        engine.compact_csr(m.ptr, m.idx, m.val, m.n, [0, 1], np.arange(m.n), m.n)
+    assert e.value.status == "NO_DEVICE"
+    with pytest.raises(engine.EngineError) as e:
+        engine.propagate_bounds(m, np.zeros(m.n, dtype=np.int32), m.lb, m.ub)
+    assert e.value.status == "NO_DEVICE"
