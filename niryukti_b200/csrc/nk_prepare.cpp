@@ -160,22 +160,11 @@ void pock_chambolle_scale(Prepared &p) {
     extra_scale(p, row, col);
 }
 
-// Hash of a row key (mapped columns, values) for duplicate-row detection; the
-// reference keys a std::map on the same vectors, so equal keys are found alike.
-struct KeyHash {
-    size_t operator()(const std::vector<std::pair<int64_t, double>> &k) const {
-        uint64_t h = 1469598103934665603ULL;
-        for (auto &e : k) {
-            uint64_t bits;
-            std::memcpy(&bits, &e.second, 8);
-            h = (h ^ uint64_t(e.first)) * 1099511628211ULL;
-            h = (h ^ bits) * 1099511628211ULL;
-        }
-        return size_t(h);
-    }
-};
-
-// KeyHash of row [b, en) of A with its columns mapped, without building the key.
+// Hash of row [b, en) of A as a duplicate-row key (its mapped columns and
+// values, in order; FNV-1a over their bits), without building the key.  The
+// reference keys a std::map on the same (column, value) vectors; a hash bucket
+// is only a shortlist here, the keys themselves are compared by same_row_key,
+// so equal keys are found alike.
 uint64_t row_key_hash(const Csr &A, const std::vector<int64_t> &map, int64_t b, int64_t en) {
     uint64_t h = 1469598103934665603ULL;
     for (auto k = b; k < en; ++k) {
