@@ -211,6 +211,48 @@ def run_cpu_child(args):
     return json.loads(out.stdout.strip().splitlines()[-1])
 
 
+def ref_gpu_child(args):
+    """The reference's own CUDA backend (src/cuda.cu built for sm_100a by
+    oracle/Makefile refcuda: cuSPARSE SpMVs, its trial kernels and graphs) on
+    the same LP: wall-clock time of advance(100) chunks, each of which ends in
+    the backend's own stream synchronisation."""
+    from oracle import oracle as orc
+    model = build_model(args)
+    be = orc.Reference(orc.REF_CUDA_SO).model(model).backend(
+        np.zeros(model.n), np.zeros(model.m), adaptive=True, device="cuda", graphs=True)
+    tau, sigma = step_sizes(model)
+    for _ in range(args.warmup):
+        be.advance(TRIALS_PER_STEP, tau, sigma)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        be.advance(TRIALS_PER_STEP, tau, sigma)
+    dt = time.perf_counter() - t0
+    print(json.dumps({"trials": args.steps * TRIALS_PER_STEP, "seconds": dt}))
+
+
+def reference_gpu(args, m, n, nnz):
+    """The reference GPU backend's iteration rate on this LP, in a child process
+    (None when its build is absent)."""
+    from oracle import oracle as orc
+    if not orc.REF_CUDA_SO.exists():
+        return None
+    cmd = [sys.executable, str(pathlib.Path(__file__).resolve()), "--ref-gpu-child",
+           "--steps", str(args.steps), "--warmup", str(args.warmup), "--scale", str(args.scale)] + \
+        (["--small"] if args.small else [])
+    try:
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+        if out.returncode != 0:
+            return {"error": out.stderr[-600:]}
+        r = json.loads(out.stdout.strip().splitlines()[-1])
+    except Exception as exc:
+        return {"error": str(exc)[-600:]}
+    it_s = r["trials"] / r["seconds"]
+    return {"impl": "reference src/cuda.cu (cuSPARSE), built for sm_100a", "iterations_per_s": it_s,
+            "spmv_GBps": it_s * iteration_spmv_bytes(m, n, nnz) / 1e9,
+            "timing": "wall clock around advance(100) chunks; each ends in the backend's own "
+                      "stream synchronisation", "trials": r["trials"], "seconds": r["seconds"]}
+
+
 def reference_arm(args, world, rank):
     if rank != 0:
         return
@@ -757,6 +799,8 @@ def engine_arm(args, world, rank, local):
             "gpu_launches": 2 * (args.steps * TRIALS_PER_STEP),
             "clocks": clocks.summary(), "accepted_trials": accepted,
             "precision_forms": forms}
+    if not args.no_ref_gpu:
+        line["reference_gpu"] = reference_gpu(args, m, n, nnz)
     if not args.no_solve:
         line["solve"] = solve_section(args)
     if not args.no_batch:
@@ -778,6 +822,9 @@ def main():
                     help="scale m, n and nnz of the config-2 generator (profiling cases)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-child", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--ref-gpu-child", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="skip the reference's own CUDA backend on the same LP")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--cpu-threads", type=int, default=os.cpu_count() or 1)
     ap.add_argument("--cpu-trials", type=int, default=5)
@@ -821,6 +868,8 @@ def main():
         ap.error("--warmup must be at least 3")
     if args.cpu_child:
         return cpu_child(args)
+    if args.ref_gpu_child:
+        return ref_gpu_child(args)
     if args.solve_child:
         return solve_child(args)
     if args.batch_only:

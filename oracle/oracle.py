@@ -23,6 +23,7 @@ HERE = pathlib.Path(__file__).resolve().parent
 ORACLE_SO = HERE / "liboracle.so"
 REF_SO = HERE / "_ref" / "libvantage_ref.so"
 BRIDGE_SO = HERE / "_ref" / "libvantage_nk.so"
+REF_CUDA_SO = HERE / "_ref" / "libvantage_cuda.so"  # the reference's own CUDA build
 
 _D = C.POINTER(C.c_double)
 _I = C.POINTER(C.c_int64)
