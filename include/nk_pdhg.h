@@ -146,6 +146,7 @@ nk_status nk_pdhg_schedule_info(nk_pdhg *h, int *a_width, int64_t *a_long, int *
 #define NK_SOLVE_ITERATION_LIMIT 3
 #define NK_SOLVE_TIME_LIMIT 4
 #define NK_SOLVE_NUMERICAL_ERROR 5
+#define NK_SOLVE_INTERRUPTED 6
 
 /* The continuous part of vantage::Model (include/vantage/vantage.hpp:26-39):
  * minimise offset + c'x + 1/2 sum q_j x_j^2 + 1/2 x'Qx
@@ -176,6 +177,9 @@ typedef struct {
     int verbose;              /* per-check line on stderr (0) */
     const double *initial_x;  /* optional, n entries */
     const double *initial_y;  /* optional, m entries */
+    const volatile int *cancel; /* optional: another thread sets *cancel != 0 to stop the
+                                   solve at its next check (INTERRUPTED) -- the reference's
+                                   Options::cancellation token (src/internal.hpp:9-11) */
 } nk_solve_options;
 
 /* vantage::Result fields of the continuous path (include/vantage/vantage.hpp:112-140). */

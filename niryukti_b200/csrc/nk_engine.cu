@@ -1847,6 +1847,7 @@ nk_status nk_solve(const nk_model *model, const nk_solve_options *o, nk_solve_re
         S.driver.graphs = o->graphs != 0;
         S.driver.index_bits = o->index_bits;
         S.driver.verbose = o->verbose != 0;
+        S.driver.cancel = o->cancel;
         S.prepare.presolve = o->presolve != 0;
         S.prepare.scaling = o->scaling_combined ? "combined" : "ruiz";
         S.prepare.scaling_passes = o->scaling_passes;

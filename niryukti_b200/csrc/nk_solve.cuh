@@ -526,6 +526,7 @@ struct DriverOptions {
     bool adaptive = true, restart = true, graphs = true;
     int index_bits = 0;
     bool verbose = false;
+    const volatile int *cancel = nullptr; // nonzero: stop at the next check (INTERRUPTED)
 };
 
 // Iterates one DeviceSolve until its device estimate reaches `target` (and, if
@@ -565,6 +566,11 @@ struct Driver {
         int stagnant = 0;
         double stagnant_ref = kInf;
         while (R.iterations < iteration_cap) {
+            // stop_requested, then the time limit, as src/solver.cpp:516-523 orders them
+            if (o.cancel && *o.cancel) {
+                R.status = NK_SOLVE_INTERRUPTED;
+                return false;
+            }
             if (since(start) >= o.time_limit) {
                 R.status = NK_SOLVE_TIME_LIMIT;
                 return false;
@@ -833,7 +839,8 @@ inline SolveReport solve(const HostModel &original, const SolveSettings &S) {
             R.verification += since(tick);
         }
         bool stopped = R.status == NK_SOLVE_TIME_LIMIT || R.status == NK_SOLVE_INFEASIBLE ||
-                       R.status == NK_SOLVE_OPTIMAL || R.iterations >= o.iteration_limit;
+                       R.status == NK_SOLVE_OPTIMAL || R.status == NK_SOLVE_INTERRUPTED ||
+                       R.iterations >= o.iteration_limit;
         if (S.refine && !stopped && best.finite) {
             // closing FP64 refinement, restarted from the best reduced-precision point
             auto bx = D->download_cols(D->best_x.p);

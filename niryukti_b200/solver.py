@@ -18,7 +18,23 @@ import numpy as np
 from .engine import NkCsr, PRECISIONS, _D, _I, _f64, _i64, check, library
 
 STATUS = {0: "OPTIMAL", 1: "INFEASIBLE", 2: "UNBOUNDED", 3: "ITERATION_LIMIT", 4: "TIME_LIMIT",
-          5: "NUMERICAL_ERROR"}
+          5: "NUMERICAL_ERROR", 6: "INTERRUPTED"}
+
+
+class CancelToken:
+    """Stops a running solve() at its next check (status INTERRUPTED) when
+    cancel() is called from another thread -- the reference's
+    Options::cancellation."""
+
+    def __init__(self):
+        self.flag = C.c_int(0)
+
+    def cancel(self):
+        self.flag.value = 1
+
+    @property
+    def cancelled(self) -> bool:
+        return bool(self.flag.value)
 ACCURACY_KEYS = ("objective", "primal", "dual", "gap", "kkt", "primal_absolute", "dual_absolute",
                  "complementarity", "lower_bound", "finite")
 
@@ -34,7 +50,7 @@ class NkSolveOptions(C.Structure):
                 ("scaling_passes", C.c_int), ("adaptive", C.c_int), ("restart", C.c_int),
                 ("graphs", C.c_int), ("index_bits", C.c_int), ("precision", C.c_int),
                 ("refine", C.c_int), ("phase_tol", C.c_double), ("verbose", C.c_int),
-                ("initial_x", _D), ("initial_y", _D)]
+                ("initial_x", _D), ("initial_y", _D), ("cancel", C.POINTER(C.c_int))]
 
 
 class NkSolveResult(C.Structure):
@@ -116,9 +132,11 @@ def default_options() -> dict:
 def solve(model, *, tol=1e-6, time_limit=60.0, iteration_limit=100000, check_every=100,
           presolve=True, scaling="ruiz", scaling_passes=5, adaptive=True, restart=True,
           cuda_graphs=True, gpu_indices="auto", matrix_precision="fp64", refine=True,
-          phase_tol=0.0, verbose=False, initial_x=None, initial_y=None) -> dict:
+          phase_tol=0.0, verbose=False, initial_x=None, initial_y=None,
+          cancel: "CancelToken | None" = None) -> dict:
     """Solve an LP / convex QP on the GPU; returns the reference's result keys
-    plus ``x`` and ``y`` (caller order, original units)."""
+    plus ``x`` and ``y`` (caller order, original units).  ``cancel``: a
+    CancelToken another thread may trigger (status INTERRUPTED)."""
     L = _bind()
     if scaling not in ("ruiz", "combined"):
         raise ValueError("scaling must be 'ruiz' or 'combined'")
@@ -141,6 +159,8 @@ def solve(model, *, tol=1e-6, time_limit=60.0, iteration_limit=100000, check_eve
     if initial_y is not None:
         iy = _f64(initial_y)
         o.initial_y = iy.ctypes.data_as(_D)
+    if cancel is not None:
+        o.cancel = C.pointer(cancel.flag)
     x = np.zeros(int(model.n))
     y = np.zeros(int(model.m))
     r = NkSolveResult()

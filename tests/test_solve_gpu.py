@@ -152,3 +152,36 @@ def test_power_law_lp_solves(solver, reference):
     ref = reference.model(model).solve(method="pdhg", device="cpu", tol=1e-4)
     assert ref["status"] == "OPTIMAL"
     objective_close(r["objective"], ref["objective"], 1e-4)
+
+
+def test_cancellation_interrupts_a_running_solve(solver):
+    """The reference's cancellation token (Options::cancellation,
+    src/internal.hpp:9-11): another thread cancels a solve that would run for
+    its whole time limit; the solve stops at its next check with status
+    INTERRUPTED and returns its best point.  A host-side failure injection:
+    nothing on the GPU is made to fail."""
+    import threading
+    import time
+    model = synth.power_law_lp(m=200000, n=400000, nnz=4000000, seed=2)
+    token = solver.CancelToken()
+    timer = threading.Timer(3.0, token.cancel)
+    t0 = time.perf_counter()
+    timer.start()
+    try:
+        r = solver.solve(model, tol=1e-9, time_limit=120.0, iteration_limit=10**9, cancel=token)
+    finally:
+        timer.cancel()
+    wall = time.perf_counter() - t0
+    assert token.cancelled
+    assert r["status"] == "INTERRUPTED"
+    assert r["iterations"] > 0
+    assert wall < 30.0  # far below the 120 s limit
+    assert np.all(np.isfinite(r["x"])) and np.all(np.isfinite(r["y"]))
+
+
+def test_cancelled_before_the_first_check(solver, golden_lp):
+    model, _ = golden_lp
+    token = solver.CancelToken()
+    token.cancel()
+    r = solver.solve(model, cancel=token)
+    assert r["status"] == "INTERRUPTED" and r["iterations"] == 0
