@@ -179,7 +179,7 @@ def linear_solve(ptr, idx, val, rhs, fp32_matrix=False, precondition=True, time_
                                     int(bool(precondition)), float(time_limit), _d(x),
                                     C.byref(ok), C.byref(late)))
     if late.value:
-        raise EngineError(3, "GPU Newton solve time-limited")
+        raise TimeoutError("GPU Newton solve time-limited")
     return x, bool(ok.value)
 
 
