@@ -290,6 +290,9 @@ def reference_arm(args, world, rank):
                                        "config-2 LP (adaptive, FP64), CpuBackend::advance"},
             "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
+    if not args.no_ref_gpu:
+        # beside the CPU arm: the reference's own CUDA build on the same LP, when built
+        line["reference_gpu"] = reference_gpu(args, m, n, nnz)
     print(json.dumps(line))
 
 
@@ -799,8 +802,6 @@ def engine_arm(args, world, rank, local):
             "gpu_launches": 2 * (args.steps * TRIALS_PER_STEP),
             "clocks": clocks.summary(), "accepted_trials": accepted,
             "precision_forms": forms}
-    if not args.no_ref_gpu:
-        line["reference_gpu"] = reference_gpu(args, m, n, nnz)
     if not args.no_solve:
         line["solve"] = solve_section(args)
     if not args.no_batch:
@@ -824,7 +825,7 @@ def main():
     ap.add_argument("--cpu-child", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--ref-gpu-child", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--no-ref-gpu", action="store_true",
-                    help="skip the reference's own CUDA backend on the same LP")
+                    help="--impl reference: skip the reference's own CUDA backend on the same LP")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--cpu-threads", type=int, default=os.cpu_count() or 1)
     ap.add_argument("--cpu-trials", type=int, default=5)
