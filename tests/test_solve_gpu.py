@@ -185,3 +185,17 @@ def test_cancelled_before_the_first_check(solver, golden_lp):
     token.cancel()
     r = solver.solve(model, cancel=token)
     assert r["status"] == "INTERRUPTED" and r["iterations"] == 0
+
+
+def test_sparse_qp_matches_reference(solver, reference):
+    """A convex QP with sparse Q = D + L L^T (the batch's QP shape), the
+    reference's 'large SPD QP, CUDA vs CPU objective' check
+    (tests/test_research.cpp:825-832): OPTIMAL, objective within
+    2 tol (1 + |f|) of the reference's CPU solve."""
+    rng = np.random.default_rng(7)
+    model = synth.batch_instance(rng, 800, qp=True, name="qp")
+    want = reference.model(model).solve(method="pdhg", device="cpu", iteration_limit=200000)
+    r = solver.solve(model, iteration_limit=200000)
+    assert want["status"] == r["status"] == "OPTIMAL"
+    assert r["kkt"] <= TOL
+    objective_close(r["objective"], want["objective"])
