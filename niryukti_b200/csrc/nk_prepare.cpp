@@ -8,6 +8,7 @@
 // long double where the reference uses it), compiled without FMA contraction,
 // so the prepared model is bit-identical to the reference's.
 #include "nk_host.hpp"
+#include <omp.h>
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -227,6 +228,10 @@ Csr build_csr(int64_t rows, int64_t cols, std::vector<Entry> e) {
     return s;
 }
 
+// Transpose with each column's entries in increasing row order (the order of
+// a sequential row sweep).  Large matrices are swept by contiguous row blocks
+// in parallel: block b places its entries of column j after those of blocks
+// before it, so the result is the sequential one entry for entry.
 Csr transpose(const Csr &a) {
     Csr t;
     t.rows = a.cols;
@@ -234,6 +239,57 @@ Csr transpose(const Csr &a) {
     t.ptr.assign(size_t(a.cols + 1), 0);
     t.index.resize(a.value.size());
     t.value.resize(a.value.size());
+    const size_t nnz = a.value.size();
+    const int blocks = omp_get_max_threads();
+    if (nnz > (1u << 20) && nnz < (size_t(1) << 32) && blocks > 1 && !g_host_serial &&
+        a.cols < (int64_t(1) << 31)) {
+        const size_t cols = size_t(a.cols);
+        std::vector<int64_t> first(size_t(blocks) + 1);
+        for (int b = 0; b <= blocks; ++b) // row blocks of about equal entry counts
+            first[size_t(b)] = int64_t(std::lower_bound(a.ptr.begin(), a.ptr.end(),
+                                                        int64_t(nnz * size_t(b) / size_t(blocks))) -
+                                       a.ptr.begin());
+        first[size_t(blocks)] = a.rows;
+        std::vector<uint32_t> count(size_t(blocks) * cols, 0);
+#pragma omp parallel for num_threads(blocks) schedule(static, 1)
+        for (int b = 0; b < blocks; ++b) {
+            uint32_t *mine = count.data() + size_t(b) * cols;
+            for (auto k = a.ptr[size_t(first[size_t(b)])]; k < a.ptr[size_t(first[size_t(b + 1)])];
+                 ++k)
+                ++mine[size_t(a.index[size_t(k)])];
+        }
+        // column lengths, column offsets, then each block's start inside each column
+#pragma omp parallel for num_threads(blocks)
+        for (int64_t jj = 0; jj < int64_t(cols); ++jj) {
+            int64_t total = 0;
+            for (int b = 0; b < blocks; ++b)
+                total += count[size_t(b) * cols + size_t(jj)];
+            t.ptr[size_t(jj) + 1] = total;
+        }
+        for (size_t j = 0; j < cols; ++j)
+            t.ptr[j + 1] += t.ptr[j];
+#pragma omp parallel for num_threads(blocks)
+        for (int64_t jj = 0; jj < int64_t(cols); ++jj) {
+            uint32_t run = 0;
+            for (int b = 0; b < blocks; ++b) {
+                const uint32_t c = count[size_t(b) * cols + size_t(jj)];
+                count[size_t(b) * cols + size_t(jj)] = run;
+                run += c;
+            }
+        }
+#pragma omp parallel for num_threads(blocks) schedule(static, 1)
+        for (int b = 0; b < blocks; ++b) {
+            uint32_t *at = count.data() + size_t(b) * cols;
+            for (int64_t i = first[size_t(b)]; i < first[size_t(b + 1)]; ++i)
+                for (auto k = a.ptr[size_t(i)]; k < a.ptr[size_t(i + 1)]; ++k) {
+                    const size_t j = size_t(a.index[size_t(k)]);
+                    const size_t p = size_t(t.ptr[j]) + at[j]++;
+                    t.index[p] = i;
+                    t.value[p] = a.value[size_t(k)];
+                }
+        }
+        return t;
+    }
     for (auto j : a.index)
         t.ptr[size_t(j + 1)]++;
     for (int64_t j = 0; j < a.cols; j++)

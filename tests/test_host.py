@@ -219,6 +219,23 @@ def test_verify_bit_exact(reference, name, safe):
         same(solver.infeasibility_bound(model, y), ref.infeasibility_bound(y), "farkas")
 
 
+def test_verify_bit_exact_threaded(reference):
+    """Above a million nonzeros the verifier's transpose is built by row blocks
+    on all host threads; the outward-rounded bound and every accuracy field
+    must still be the reference's, bit for bit."""
+    model = synth.power_law_lp(m=100000, n=200000, nnz=2000000, seed=4, len_hi=3000)
+    rng = np.random.default_rng(5)
+    x = rng.uniform(0, 5, model.n)
+    y = rng.normal(size=model.m) * 1e-2
+    ref = reference.model(model)
+    for safe in (True, False):
+        a = solver.verify(model, x, y, safe)
+        b = ref.verify(x, y, safe)
+        same([a[k] for k in solver.ACCURACY_KEYS], [b[k] for k in solver.ACCURACY_KEYS],
+             f"accuracy safe={safe}")
+    same(solver.infeasibility_bound(model, y), ref.infeasibility_bound(y), "farkas")
+
+
 def test_invalid_model_rejected():
     m = tiny(2, 1, [(0, 0, 1.0)])
     m.lb[0] = 5.0
