@@ -485,15 +485,61 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
         for (auto k = b; k < en; k++)
             kept_entries += map[size_t(src.A.index[size_t(k)])] >= 0;
     }
-    std::vector<Entry> e;
-    e.reserve(kept_entries);
-    for (size_t r = 0; r < p.rows.size(); ++r) {
-        const int64_t i = p.rows[r];
-        for (auto k = src.A.ptr[size_t(i)]; k < src.A.ptr[size_t(i + 1)]; k++)
-            if (map[size_t(src.A.index[size_t(k)])] >= 0)
-                e.push_back({int64_t(r), map[size_t(src.A.index[size_t(k)])], src.A.value[size_t(k)]});
+    // The kept entries.  When every kept row's columns strictly increase (a
+    // canonical CSR: the map keeps column order), Sparse::build would only drop
+    // zero values, so the CSR is written directly, rows in parallel; otherwise
+    // the entries go through build_csr (sort, merge, drop zeros).
+    const int64_t kept_rows = int64_t(p.rows.size());
+    std::vector<int64_t> row_len(static_cast<size_t>(kept_rows), 0);
+    int canonical = 1;
+#pragma omp parallel for reduction(min : canonical) if (kept_entries > 200000 && !g_host_serial)
+    for (int64_t r = 0; r < kept_rows; ++r) {
+        const int64_t i = p.rows[size_t(r)];
+        int64_t last = -1, len = 0;
+        for (auto k = src.A.ptr[size_t(i)]; k < src.A.ptr[size_t(i + 1)]; k++) {
+            const int64_t j = map[size_t(src.A.index[size_t(k)])];
+            if (j < 0)
+                continue;
+            if (j <= last)
+                canonical = 0;
+            last = j;
+            len += src.A.value[size_t(k)] != 0;
+        }
+        row_len[size_t(r)] = len;
     }
-    m.A = build_csr(int64_t(m.rl.size()), nk, std::move(e));
+    if (canonical) {
+        Csr &A = m.A;
+        A.rows = kept_rows;
+        A.cols = nk;
+        A.ptr.assign(size_t(kept_rows + 1), 0);
+        for (int64_t r = 0; r < kept_rows; ++r)
+            A.ptr[size_t(r + 1)] = A.ptr[size_t(r)] + row_len[size_t(r)];
+        A.index.resize(size_t(A.ptr.back()));
+        A.value.resize(size_t(A.ptr.back()));
+#pragma omp parallel for if (kept_entries > 200000 && !g_host_serial)
+        for (int64_t r = 0; r < kept_rows; ++r) {
+            const int64_t i = p.rows[size_t(r)];
+            int64_t at = A.ptr[size_t(r)];
+            for (auto k = src.A.ptr[size_t(i)]; k < src.A.ptr[size_t(i + 1)]; k++) {
+                const int64_t j = map[size_t(src.A.index[size_t(k)])];
+                if (j >= 0 && src.A.value[size_t(k)] != 0) {
+                    A.index[size_t(at)] = j;
+                    A.value[size_t(at++)] = src.A.value[size_t(k)];
+                }
+            }
+        }
+    } else {
+        std::vector<Entry> e;
+        e.reserve(kept_entries);
+        for (size_t r = 0; r < p.rows.size(); ++r) {
+            const int64_t i = p.rows[r];
+            for (auto k = src.A.ptr[size_t(i)]; k < src.A.ptr[size_t(i + 1)]; k++)
+                if (map[size_t(src.A.index[size_t(k)])] >= 0)
+                    e.push_back({int64_t(r), map[size_t(src.A.index[size_t(k)])],
+                                 src.A.value[size_t(k)]});
+        }
+        m.A = build_csr(int64_t(m.rl.size()), nk, std::move(e));
+    }
     p.column_scale.assign(size_t(nk), 1);
     p.row_scale.assign(m.rl.size(), 1);
     if (o.scaling == "combined" && o.scaling_passes > 0)
