@@ -41,8 +41,13 @@ bool representable(double before, double after) {
 void extra_scale(Prepared &p, const std::vector<double> &row, std::vector<double> col) {
     HostModel &m = p.model;
     const bool par = m.A.value.size() > 200000 && !g_host_serial;
-#pragma omp parallel for schedule(dynamic, 1024) if (par)
-    for (int64_t ii = 0; ii < int64_t(row.size()); ii++) {
+    // A side whose factors are all 1 changes nothing (x * 1 == x, and every
+    // representability test passes): the Ruiz passes scale rows and columns in
+    // separate calls, so each call skips the other side's loops.
+    const bool rows_one = std::all_of(row.begin(), row.end(), [](double f) { return f == 1; });
+    const bool cols_one = std::all_of(col.begin(), col.end(), [](double f) { return f == 1; });
+#pragma omp parallel for schedule(dynamic, 1024) if (par && !rows_one)
+    for (int64_t ii = 0; ii < (rows_one ? 0 : int64_t(row.size())); ii++) {
         const size_t i = size_t(ii);
         double f = row[i];
         bool safe = representable(p.row_scale[i], p.row_scale[i] * f) &&
@@ -57,6 +62,8 @@ void extra_scale(Prepared &p, const std::vector<double> &row, std::vector<double
         for (int64_t k = m.A.ptr[i]; k < m.A.ptr[i + 1]; k++)
             m.A.value[k] *= f;
     }
+    if (cols_one)
+        return;
 #pragma omp parallel for if (par)
     for (int64_t jj = 0; jj < int64_t(col.size()); jj++) {
         const size_t j = size_t(jj);
@@ -427,6 +434,7 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
     }
     // first occurrence (prepared row) of each key, by hash; keys are compared in full
     std::unordered_multimap<uint64_t, size_t> duplicate_rows;
+    duplicate_rows.reserve(size_t(mrows));
     size_t kept_entries = 0;
     for (int64_t i = 0; i < mrows; i++) {
         const char v = verdict[size_t(i)];
