@@ -1,5 +1,5 @@
 #!/usr/bin/env python
-"""Benchmark of the PDHG hot path on the config-2 LP (m=1e6, n=2e6, 20M nnz,
+"""Benchmark of the PDHG hot path on the power-law LP (m=1e6, n=2e6, 20M nnz,
 power-law rows), one B200.
 
 A *step* is one check interval of the reference's driver: 100 PDHG trials
@@ -153,7 +153,7 @@ def dist_setup():
 
 
 def build_model(args):
-    """Config 2 (m=1e6, n=2e6, nnz=2e7), or the same generator scaled by
+    """The power-law LP (m=1e6, n=2e6, nnz=2e7), or the same generator scaled by
     --scale (profiling captures use a smaller, still larger-than-L2 case)."""
     from niryukti_b200 import synth
     f = 0.1 if args.small else args.scale
@@ -287,7 +287,7 @@ def reference_arm(args, world, rank):
             "iterations_per_s": rate,
             "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": kind,
                              "sample": f"{args.steps} steps x {per} PDHG trials of the "
-                                       "config-2 LP (adaptive, FP64), CpuBackend::advance"},
+                                       "power-law LP (adaptive, FP64), CpuBackend::advance"},
             "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     if not args.no_ref_gpu:
@@ -348,7 +348,7 @@ def solve_child(args):
 
 def solve_section(args):
     """Time to 1e-6 relative KKT through the public solve API (host model in,
-    certified x, y out): config 1 to tolerance, config 2 within a budget, each
+    certified x, y out): the 2,000 x 5,000 LP to tolerance, the power-law LP within a budget, each
     beside the reference's own CPU solve of the same LP."""
     from niryukti_b200 import solver
     res = {}
@@ -393,7 +393,7 @@ def solve_section(args):
     return res
 
 
-# ---------------------------------------------------------------- batch (config 4)
+# ---------------------------------------------------------------- batch (512 uneven LP/QP instances)
 def batch_models(args):
     from niryukti_b200 import synth
     return synth.batch_instances(count=args.batch_count, m_lo=500, m_hi=args.batch_m_hi,
@@ -401,7 +401,7 @@ def batch_models(args):
 
 
 def batch_section(args):
-    """Config 4: 512 uneven LP/QP instances (m log-uniform in [500, 50000],
+    """The batch: 512 uneven LP/QP instances (m log-uniform in [500, 50000],
     n = 2m, 20% QPs) solved to 1e-6 relative KKT by the batched engine (FP32
     matrices, FP64 iterates and reductions), beside the plain FP64 solve run
     instance by instance on the same GPU (a stratified sample, timed one by
@@ -423,7 +423,7 @@ def batch_section(args):
         g0 = time.perf_counter()
         for k, it in enumerate(items):
             if not eng.admit(it, k):
-                raise MemoryError("config-4 batch does not fit the device budget")
+                raise MemoryError("the 512-instance batch does not fit the device budget")
         info = eng.info()
         results, finish_t = {}, {}
         while len(results) < len(models):
@@ -489,7 +489,7 @@ def batch_section(args):
 
 
 def batch_throughput(args):
-    """Trial throughput of the config-4 batch (no solve): admit every
+    """Trial throughput of the 512-instance batch (no solve): admit every
     instance, run one check interval (this also autotunes the kernels), then
     time --batch-trials PDHG trials of the whole batch with CUDA events."""
     from concurrent.futures import ThreadPoolExecutor
@@ -501,7 +501,7 @@ def batch_throughput(args):
             items = list(pool.map(eng.prepare, models))
         for k, it in enumerate(items):
             if not eng.admit(it, k):
-                raise MemoryError("config-4 batch does not fit the device budget")
+                raise MemoryError("the 512-instance batch does not fit the device budget")
         eng.step(1)
         ms, bts = eng.time_trials(args.batch_trials)
         kp, kd = eng.kernel_times()
@@ -514,10 +514,10 @@ def batch_throughput(args):
             "variants": {"primal": info["primal_variant"], "dual": info["dual_variant"]}}
 
 
-# ---------------------------------------------------------------- serving (config 5)
+# ---------------------------------------------------------------- serving (Poisson stream)
 def serve_section(args):
-    """Config 5: Poisson arrivals at --serve-rate requests/s for --serve-seconds,
-    each request drawn from a pool of config-4-style instances with m
+    """The served stream: Poisson arrivals at --serve-rate requests/s for --serve-seconds,
+    each request drawn from a pool of instances of the uneven LP/QP mix with m
     log-uniform in [500, 200000]; served by continuous batching (admission by
     device-memory footprint under a 150 GB budget), and by the plain FP64
     solve one request at a time on the same arrival stream.  Reported over the
@@ -645,7 +645,7 @@ def time_form(model, precision, steps, warmup, profile_trials):
 
 
 def config3_section(args):
-    """Config 3: the block-angular planning LP (64 blocks of 20,000 x 40,000
+    """The block-angular planning LP (64 blocks of 20,000 x 40,000
     with 6 nonzeros per column, 2,000 linking rows over 5% of all columns
     each), iteration rate in FP64 and with FP32 matrices."""
     import torch
@@ -724,7 +724,7 @@ def engine_arm(args, world, rank, local):
     peak = float(peaks.get("hbm_gbs", 6650.0))
     traffic, traffic_source = args.traffic, "--traffic" if args.traffic else None
     if traffic is None and args.precision == "fp64" and not args.small and args.scale == 1.0:
-        # DRAM bytes per launch from the ncu capture of the config-2 shape at half
+        # DRAM bytes per launch from the ncu capture of the power-law LP at half
         # size (profiles/fused_pdhg_kernels_config2_scaled_half.md: read + write),
         # scaled by 2: every unit (nonzeros, rows, columns) doubles
         traffic = {"primal_kernel": 2 * 181.32e6, "dual_kernel": 2 * 166.24e6}[top]
@@ -778,7 +778,7 @@ def engine_arm(args, world, rank, local):
             c = run_cpu_child(args)
             cpu = {"value": c["rate"] * iteration_spmv_bytes(m, n, nnz) / 1e9, "unit": "GB/s",
                    "cores": c["threads"], "kind": c["kind"],
-                   "sample": f"{c['done']} adaptive FP64 PDHG trials of the same config-2 LP in "
+                   "sample": f"{c['done']} adaptive FP64 PDHG trials of the same power-law LP in "
                              f"{c['dt']:.1f} s (CpuBackend::advance, OMP threads {c['threads']})",
                    "iterations_per_s": c["rate"]}
         except Exception as exc:  # reported, never silently replaced
@@ -820,7 +820,7 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "fp32"])
     ap.add_argument("--small", action="store_true", help="10x smaller instance (testing)")
     ap.add_argument("--scale", type=float, default=1.0,
-                    help="scale m, n and nnz of the config-2 generator (profiling cases)")
+                    help="scale m, n and nnz of the power-law generator (profiling cases)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-child", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--ref-gpu-child", action="store_true", help=argparse.SUPPRESS)
@@ -834,18 +834,18 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-solve", action="store_true", help="skip the time-to-tolerance solves")
     ap.add_argument("--solve-seconds", type=float, default=60.0,
-                    help="time budget of the config-2 solve on the GPU")
+                    help="time budget of the power-law LP solve on the GPU")
     ap.add_argument("--cpu-solve-seconds", type=float, default=30.0,
-                    help="time budget of the reference's config-2 CPU solve")
+                    help="time budget of the reference's CPU solve of the power-law LP")
     ap.add_argument("--solve-child", action="store_true", help=argparse.SUPPRESS)
-    ap.add_argument("--no-batch", action="store_true", help="skip the config-4 batched solves")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 512-instance batched solves")
     ap.add_argument("--batch-only", action="store_true",
-                    help="print only the config-4 batched-solve section")
+                    help="print only the 512-instance batched-solve section")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--batch-trials", type=int, default=0,
                     help="with --batch-only: time this many batch trials instead of solving")
     ap.add_argument("--serve", action="store_true",
-                    help="print only the config-5 served-stream section")
+                    help="print only the served-stream section")
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-drain", type=float, default=60.0)
@@ -858,9 +858,9 @@ def main():
     ap.add_argument("--batch-cpu-sample", type=int, default=4,
                     help="smallest sampled instances also solved by the reference on the CPU")
     ap.add_argument("--no-forms", action="store_true",
-                    help="skip the FP32-matrix forms of the config-2 iteration rate")
+                    help="skip the FP32-matrix forms of the power-law LP iteration rate")
     ap.add_argument("--config3", action="store_true",
-                    help="print only the config-3 block-angular iteration-rate section")
+                    help="print only the block-angular LP iteration-rate section")
     ap.add_argument("--config3-blocks", type=int, default=64)
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per launch of the top kernel from an ncu capture")

@@ -11,12 +11,12 @@ Bounds and row intervals follow the reference ``Model`` conventions
 ``-inf/+inf`` for a missing side, equality rows have ``rl == ru``.
 
 Generators:
-  * :func:`random_lp`     - config 1 shape: m equality rows, n columns, a fixed number of
+  * :func:`random_lp`     - the small equality LP (2,000 x 5,000 in the benchmark): m equality rows, n columns, a fixed number of
                             nonzeros per column at distinct random rows.
-  * :func:`power_law_lp`  - config 2 shape: power-law row lengths, log-uniform row factors,
+  * :func:`power_law_lp`  - the 20M-nonzero power-law LP: power-law row lengths, log-uniform row factors,
                             half equality / half <= rows, 10% free columns.
-  * :func:`block_angular_lp` - config 3 shape: diagonal blocks plus dense-ish linking rows.
-  * :func:`batch_instances`  - config 4/5 shape: uneven LP/QP mix, n = 2m, 4-8 nnz per column,
+  * :func:`block_angular_lp` - the block-angular planning LP: diagonal blocks plus dense-ish linking rows.
+  * :func:`batch_instances`  - the uneven LP/QP instance mix of the batch and the served stream: uneven LP/QP mix, n = 2m, 4-8 nnz per column,
                             QPs with Q = D + L L^T (D on the diagonal shorthand ``q``).
 """
 from __future__ import annotations
@@ -126,7 +126,7 @@ def _names_free(model: Model) -> Model:
 
 def random_lp(m: int = 2000, n: int = 5000, per_col: int = 5, seed: int = 1,
               x_hi: float = 10.0) -> Model:
-    """Config 1 shape: m equality rows, n columns, ``per_col`` nonzeros per column at
+    """The small equality LP: m equality rows, n columns, ``per_col`` nonzeros per column at
     uniformly random distinct rows, values N(0,1); x0 ~ U[0,x_hi]; b = A x0;
     0 <= x <= x_hi; c ~ N(0,1)."""
     rng = np.random.default_rng(seed)
@@ -172,7 +172,7 @@ def power_law_exponent(mean: float, lo: int, hi: int) -> float:
 def power_law_lp(m: int = 1_000_000, n: int = 2_000_000, nnz: int = 20_000_000,
                  seed: int = 2, len_lo: int = 2, len_hi: int = 5000,
                  free_frac: float = 0.10, x_hi: float = 5.0) -> Model:
-    """Config 2 shape.
+    """The power-law LP (1,000,000 x 2,000,000, 20M nonzeros at the defaults).
 
     Row lengths follow a discrete power law on [len_lo, len_hi] whose exponent is
     chosen so the mean is nnz/m, then adjusted by +-1 on random rows to sum to
@@ -256,7 +256,7 @@ def transpose(model_or_ptr, idx=None, val=None, m=None, n=None):
 def block_angular_lp(blocks: int = 64, block_rows: int = 20_000, block_cols: int = 40_000,
                      per_col: int = 6, linking_rows: int = 2000, linking_frac: float = 0.05,
                      seed: int = 3, x_hi: float = 10.0, box_hi: float = 20.0) -> Model:
-    """Config 3 shape: ``blocks`` diagonal blocks of block_rows x block_cols with
+    """The block-angular planning LP: ``blocks`` diagonal blocks of block_rows x block_cols with
     ``per_col`` nonzeros per column, plus ``linking_rows`` rows each touching
     ``linking_frac`` of all columns.  Values U[0.1,2], negated with probability
     0.3.  Block rows are equalities at x0 ~ U[0,x_hi]; linking rows are <= rows
@@ -340,7 +340,7 @@ def sparse_qp_terms(rng, n: int, rank: int = 4, sigma: float = 0.1):
 
 
 def batch_instance(rng, m: int, qp: bool, x_hi: float = 10.0, name: str = "inst") -> Model:
-    """One config-4/5 instance: m equality rows at x0 ~ U[0,x_hi], n = 2m columns,
+    """One instance of the uneven LP/QP mix: m equality rows at x0 ~ U[0,x_hi], n = 2m columns,
     each column with 4-8 nonzeros (uniform) at distinct random rows, values N(0,1),
     bounds [0, x_hi], c ~ N(0,1); QPs add Q = D + L L^T."""
     n = 2 * m
@@ -365,7 +365,8 @@ def batch_instance(rng, m: int, qp: bool, x_hi: float = 10.0, name: str = "inst"
 
 def batch_instances(count: int = 512, m_lo: int = 500, m_hi: int = 50_000, qp_frac: float = 0.2,
                     seed: int = 4) -> list:
-    """Config 4 (and, with m_hi=200000, config 5) instance list: m log-uniform on
+    """The uneven LP/QP mix (512 instances with m up to 50,000 for the batch; m up to
+    200,000 for the served stream): m log-uniform on
     [m_lo, m_hi], a fraction ``qp_frac`` of convex QPs."""
     rng = np.random.default_rng(seed)
     ms = np.exp(rng.uniform(math.log(m_lo), math.log(m_hi), count)).astype(np.int64)

@@ -31,7 +31,7 @@ def solver(gpu):
     return s
 
 
-def test_solve_config1_lp(solver, oracle):
+def test_solve_small_random_lp(solver, oracle):
     model = synth.random_lp(m=2000, n=5000, per_col=5, seed=1)
     r = solver.solve(model, tol=TOL)
     assert r["status"] == "OPTIMAL", r
