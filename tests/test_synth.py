@@ -1,0 +1,99 @@
+"""The seeded workload generators and the benchmark's byte counts (CPU only).
+
+The generators stand in for data: each instance must be a valid canonical CSR,
+feasible at its planted point x0, and reproducible from its seed.  The byte
+formulas are the numerators of the reported bandwidths."""
+import sys
+import pathlib
+
+import numpy as np
+import pytest
+
+from niryukti_b200 import synth
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+
+
+def _canonical(m):
+    assert m.ptr[0] == 0 and m.ptr[-1] == m.idx.size == m.val.size
+    assert np.all(np.diff(m.ptr) >= 0)
+    assert np.all((m.idx >= 0) & (m.idx < m.n))
+    rows = np.repeat(np.arange(m.m), np.diff(m.ptr))
+    key = rows * m.n + m.idx
+    assert np.all(np.diff(key) > 0), "columns strictly increase within each row"
+    assert np.all(m.val != 0) and np.all(np.isfinite(m.val))
+
+
+def _feasible_at(m, x0, slack=1e-7):
+    ax = synth.csr_matvec(m.ptr, m.idx, m.val, x0, m.m)
+    scale = 1 + np.abs(ax)
+    assert np.all(ax >= m.rl - slack * scale) and np.all(ax <= m.ru + slack * scale)
+    assert np.all(x0 >= m.lb) and np.all(x0 <= m.ub)
+
+
+def test_power_law_lp_shape_and_feasibility():
+    m = synth.power_law_lp(m=20000, n=40000, nnz=400000, seed=3)
+    _canonical(m)
+    assert m.nnz == 400000
+    lens = np.diff(m.ptr)
+    assert lens.min() >= 2 and lens.max() <= 5000
+    assert np.isinf(m.lb).mean() == pytest.approx(0.10, abs=0.01)  # free columns
+    assert np.all(m.rl[: m.m // 2] == m.ru[: m.m // 2])             # equality half
+    assert np.all(np.isinf(m.rl[m.m // 2:]))                         # <= half
+    _feasible_at(m, m.x0)
+
+
+def test_block_angular_lp_structure():
+    blocks, rows_b, cols_b, link = 4, 500, 1000, 20
+    m = synth.block_angular_lp(blocks=blocks, block_rows=rows_b, block_cols=cols_b,
+                               linking_rows=link)
+    _canonical(m)
+    mb = blocks * rows_b
+    assert m.m == mb + link and m.n == blocks * cols_b
+    for r in range(0, mb, 97):  # block rows touch only their block's columns
+        cols = m.idx[m.ptr[r]:m.ptr[r + 1]]
+        assert np.all(cols // cols_b == r // rows_b)
+    per_link = int(round(0.05 * m.n))
+    assert np.all(np.diff(m.ptr)[mb:] == per_link)
+    assert np.all(np.abs(m.val) >= 0.1) and np.all(np.abs(m.val) <= 2.0)
+    assert np.all(np.isinf(m.rl[mb:])) and np.all(m.rl[:mb] == m.ru[:mb])
+    # feasible at the point the rows were built from: inside the box [0, 20]
+    assert np.all(m.lb == 0) and np.all(m.ub == 20)
+
+
+def test_generators_are_reproducible():
+    a = synth.power_law_lp(m=5000, n=10000, nnz=100000, seed=9)
+    b = synth.power_law_lp(m=5000, n=10000, nnz=100000, seed=9)
+    assert np.array_equal(a.idx, b.idx) and np.array_equal(a.val, b.val)
+    c = synth.batch_instances(count=6, m_lo=50, m_hi=300, qp_frac=0.5, seed=4)
+    d = synth.batch_instances(count=6, m_lo=50, m_hi=300, qp_frac=0.5, seed=4)
+    for u, v in zip(c, d):
+        assert np.array_equal(u.val, v.val) and np.array_equal(u.c, v.c)
+
+
+def test_batch_instances_qp_terms_are_symmetric():
+    for m in synth.batch_instances(count=8, m_lo=50, m_hi=300, qp_frac=0.5, seed=2):
+        _canonical(m)
+        _feasible_at(m, m.x0)
+        assert m.n == 2 * m.m
+        if m.qptr is None:
+            continue
+        q = np.zeros((m.n, m.n))
+        rows = np.repeat(np.arange(m.n), np.diff(m.qptr))
+        q[rows, m.qidx] = m.qval
+        assert np.array_equal(q, q.T)
+        assert np.all(np.linalg.eigvalsh(q) >= -1e-9)  # convex
+
+
+def test_benchmark_byte_counts():
+    sys.path.insert(0, str(ROOT))
+    import bench
+    m, n, nnz = 1_000_000, 2_000_000, 20_000_000
+    # one SpMV: matrix once (8 B value + 4 B index), offsets, input and output vectors
+    assert bench.spmv_bytes(m, n, nnz) == nnz * 12 + (m + 1) * 4 + n * 8 + m * 8
+    assert bench.iteration_spmv_bytes(m, n, nnz) == 268_000_004 + 272_000_004
+    primal, dual = bench.fused_kernel_bytes(m, n, nnz)
+    assert primal == 384_000_004 and dual == 324_000_004  # an LP's q is not read
+    primal_q, _ = bench.fused_kernel_bytes(m, n, nnz, diag_q=True)
+    assert primal_q == primal + 8 * n
+    assert bench.iteration_spmv_bytes(m, n, nnz, s_v=4) == 188_000_004 + 192_000_004
