@@ -327,11 +327,16 @@ class SolveService:
                 fut.set_result(r)
 
 
-def make_server(service: SolveService, host="127.0.0.1", port=8000, max_time=600.0):
+def make_server(service: SolveService, host="127.0.0.1", port=8000, max_time=600.0,
+                max_pending=None):
     """HTTP front door: POST /v1/solve as in python/niryukti/service.py:40-71
     (inline native JSON model, options {device, method, tol, time_limit,
     threads, iterations}); the CLI subprocess and worker cap are replaced by
-    the batched engine."""
+    the batched engine.  max_pending (optional) bounds the requests in flight:
+    beyond it a request is answered 429, as the reference answers when all its
+    solver workers are occupied (service.py:63-64)."""
+    pending = [0]
+    lock = threading.Lock()
 
     class Handler(BaseHTTPRequestHandler):
         def log_message(self, *args):
@@ -372,9 +377,19 @@ def make_server(service: SolveService, host="127.0.0.1", port=8000, max_time=600
                 if not 0 < tl <= max_time:
                     raise ValueError("Time limit exceeds API resource policy")
                 model = model_from_json(data["model"])
-                fut = service.submit(model, iteration_limit=options.get("iterations"),
-                                     time_limit=tl)
-                r = fut.result()
+                with lock:
+                    full = max_pending is not None and pending[0] >= max_pending
+                    if not full:
+                        pending[0] += 1
+                if full:
+                    return self.send(429, {"error": "All solver slots are occupied"})
+                try:
+                    fut = service.submit(model, iteration_limit=options.get("iterations"),
+                                         time_limit=tl)
+                    r = fut.result()
+                finally:
+                    with lock:
+                        pending[0] -= 1
                 out = result_json(model, r)
                 out["latency_seconds"] = r["latency_s"]
                 out["queue_seconds"] = r["queue_s"]
