@@ -192,20 +192,24 @@ class SolveService:
 
     def __init__(self, *, memory_budget=150e9, matrix_precision="mixed", tol=1e-6,
                  iteration_limit=100000, time_limit=600.0, check_every=100,
-                 prepare_workers=8, autotune=True, max_active_nnz=16_000_000):
+                 prepare_workers=8, autotune=True, max_active_nnz=16_000_000, engine=None):
         """memory_budget: device bytes for resident instances (admission by
         footprint).  max_active_nnz: work cap of the running batch (nonzeros
         of A and Q over the admitted instances).  A batch trial over 16 M
         nonzeros already keeps the GPU's memory system busy (about 0.2 ms per
         trial); admitting more work makes every trial longer without raising
-        throughput, so admitted instances would only finish later."""
+        throughput, so admitted instances would only finish later.  engine
+        (optional): an object with the BatchEngine methods the scheduler uses
+        (prepare_with, admit, step, result, info, close) in place of a new
+        BatchEngine -- e.g. a stand-in that exercises the scheduling on a host
+        without a GPU."""
         self.tol = tol
         self.max_active_nnz = max_active_nnz
         self._active_nnz = 0
         self.limits = dict(iteration_limit=iteration_limit, time_limit=time_limit)
-        self.engine = nb.BatchEngine(tol=tol, matrix_precision=matrix_precision,
-                                     memory_budget=memory_budget, check_every=check_every,
-                                     autotune=autotune, **self.limits)
+        self.engine = engine if engine is not None else nb.BatchEngine(
+            tol=tol, matrix_precision=matrix_precision, memory_budget=memory_budget,
+            check_every=check_every, autotune=autotune, **self.limits)
         self.precision = matrix_precision
         self.prefetch = max(2 * prepare_workers, 32)  # prepared requests kept ahead
         self._incoming = collections.deque()  # (id, model, options, future, arrival)
@@ -257,7 +261,12 @@ class SolveService:
             with self._cv:
                 self._preparing -= 1
                 if err is None:
-                    self._ready.append((ident, item, fut, arrival, model.nnz + model.qnnz))
+                    # prepared requests wait in arrival order, whichever worker finished first
+                    entry = (ident, item, fut, arrival, model.nnz + model.qnnz)
+                    at = len(self._ready)
+                    while at > 0 and self._ready[at - 1][0] > ident:
+                        at -= 1
+                    self._ready.insert(at, entry)
                 self._cv.notify_all()
             if err is not None:
                 fut.set_exception(err)
@@ -295,7 +304,7 @@ class SolveService:
                 ready = list(self._ready)
             # admission in arrival order, while the memory budget and the work
             # cap allow (an instance larger than the cap runs alone)
-            admitted = 0
+            admitted = set()
             for ident, item, fut, arrival, nnz in ready:
                 if self._running and self._active_nnz + nnz > self.max_active_nnz:
                     break
@@ -303,17 +312,19 @@ class SolveService:
                     break
                 self._running[ident] = (fut, arrival, time.perf_counter(), nnz)
                 self._active_nnz += nnz
-                admitted += 1
-            with self._cv:
-                for _ in range(admitted):
-                    self._ready.popleft()
-                if admitted:
+                admitted.add(ident)
+            if admitted:
+                # by identity: a worker may have inserted an earlier arrival meanwhile
+                with self._cv:
+                    self._ready = collections.deque(e for e in self._ready
+                                                    if e[0] not in admitted)
                     self._cv.notify_all()  # room to prepare more
             if not self._running:
                 if ready:  # the head does not fit even an empty batch
                     ident, item, fut, _, _ = ready[0]
                     with self._cv:
-                        self._ready.popleft()
+                        self._ready = collections.deque(e for e in self._ready
+                                                        if e[0] != ident)
                     item.free()
                     fut.set_exception(MemoryError("model exceeds the service's memory budget"))
                 continue

@@ -4,8 +4,9 @@ The HTTP layer (python/niryukti/service.py:40-71 in the reference) validates a
 request, turns the native JSON model into a Model, submits it and answers with
 the reference's result keys.  Here the engine is replaced by a fake service
 whose solves finish only when the test releases them, so saturation (429),
-validation errors (400, 404, 413) and the JSON round trip are exercised without
-a GPU: failures are injected on the host."""
+validation errors (400, 404) and the JSON round trip are exercised without a
+GPU: failures are injected on the host.  The scheduler of SolveService is run
+the same way, on a stand-in engine."""
 import json
 import threading
 import time
@@ -129,3 +130,134 @@ def test_native_json_round_trip():
     d["sense"] = "max"
     mx = serve.model_from_json(d)
     assert np.array_equal(mx.c, -m.c) and getattr(mx, "sense", 1.0) == -1.0
+
+
+# ---------------------------------------------------------------- the scheduler
+class FakeItem:
+    def __init__(self, model, opts):
+        self.model, self.opts, self.freed = model, opts, False
+        self.bytes = float(model.n)  # footprint: one unit per column
+
+    def free(self):
+        self.freed = True
+
+
+class FakeEngine:
+    """The BatchEngine surface the scheduler uses: admission by a byte budget,
+    and every check interval finishes the oldest running instance."""
+
+    def __init__(self, budget):
+        self.budget, self.used = budget, 0.0
+        self.running, self.admitted, self.closed = [], [], False
+        self.lock = threading.Lock()
+
+    def prepare_with(self, model, opts):
+        if model.n == 0:
+            raise ValueError("empty model")  # a presolve-time failure
+        return FakeItem(model, opts)
+
+    def admit(self, item, ident):
+        with self.lock:
+            if self.used + item.bytes > self.budget:
+                return False
+            self.used += item.bytes
+            self.running.append((ident, item))
+            self.admitted.append(ident)
+            return True
+
+    def step(self, checks=1):
+        time.sleep(0.005)
+        with self.lock:
+            if not self.running:
+                return []
+            ident, item = self.running.pop(0)
+            self.used -= item.bytes
+            return [ident]
+
+    def result(self, ident):
+        return {"status": "OPTIMAL", "ident": ident}
+
+    def info(self):
+        return {"active": len(self.running), "used_bytes": self.used}
+
+    def close(self):
+        self.closed = True
+
+
+def _lp(n):
+    from niryukti_b200 import synth
+    return synth.random_lp(m=n // 2, n=n, per_col=1, seed=n)
+
+
+def test_scheduler_admits_in_arrival_order_under_the_budget():
+    """FIFO admission under the memory budget: requests wait for memory
+    (queue_s > 0), are admitted in arrival order, and every future resolves."""
+    eng = FakeEngine(budget=250.0)
+    svc = serve.SolveService(engine=eng, prepare_workers=1)  # prepared in arrival order
+    try:
+        models = [_lp(100) for _ in range(6)]  # at most two fit at once
+        futs = [svc.submit(m) for m in models]
+        res = [f.result(timeout=30) for f in futs]
+    finally:
+        svc.close()
+    assert eng.admitted == list(range(6))
+    assert [r["ident"] for r in res] == list(range(6))
+    assert max(r["queue_s"] for r in res) > 0
+    assert all(r["latency_s"] >= r["queue_s"] >= 0 for r in res)
+    assert eng.closed
+
+
+def test_scheduler_work_cap_runs_one_at_a_time():
+    eng = FakeEngine(budget=1e9)
+    svc = serve.SolveService(engine=eng, prepare_workers=1, max_active_nnz=1)
+    try:
+        futs = [svc.submit(_lp(60)) for _ in range(4)]
+        [f.result(timeout=30) for f in futs]
+        # with a one-nonzero work cap no two instances ever ran together
+        assert eng.admitted == list(range(4))
+    finally:
+        svc.close()
+
+
+def test_scheduler_reports_failures_through_the_future():
+    """A request larger than the whole budget fails with MemoryError and one
+    whose preparation raises fails with that error; the others still finish."""
+    import pytest
+    eng = FakeEngine(budget=150.0)
+    svc = serve.SolveService(engine=eng, prepare_workers=1)
+    try:
+        too_big = svc.submit(_lp(400))
+        fine = svc.submit(_lp(100))
+        with pytest.raises(MemoryError):
+            too_big.result(timeout=30)
+        assert fine.result(timeout=30)["status"] == "OPTIMAL"
+        from niryukti_b200 import synth
+        empty = synth.Model(m=0, n=0, ptr=np.zeros(1, dtype=np.int64),
+                            idx=np.zeros(0, dtype=np.int64), val=np.zeros(0), c=np.zeros(0),
+                            q=np.zeros(0), lb=np.zeros(0), ub=np.zeros(0), rl=np.zeros(0),
+                            ru=np.zeros(0))
+        with pytest.raises(ValueError, match="empty model"):
+            svc.submit(empty).result(timeout=30)
+    finally:
+        svc.close()
+
+
+def test_scheduler_with_out_of_order_preparation():
+    """Four prepare workers finish out of arrival order: every request is
+    admitted exactly once and every future resolves once."""
+    import random
+
+    class SlowPrepare(FakeEngine):
+        def prepare_with(self, model, opts):
+            time.sleep(random.Random(model.n).uniform(0, 0.02))
+            return super().prepare_with(model, opts)
+
+    eng = SlowPrepare(budget=400.0)
+    svc = serve.SolveService(engine=eng, prepare_workers=4)
+    try:
+        futs = [svc.submit(_lp(100 + 2 * k)) for k in range(24)]
+        res = [f.result(timeout=60) for f in futs]
+    finally:
+        svc.close()
+    assert sorted(eng.admitted) == list(range(24))
+    assert [r["ident"] for r in res] == list(range(24))
