@@ -73,6 +73,10 @@ nk_status nk_pdhg_create(const nk_csr *A, const nk_csr *Q, const double *c, cons
                          nk_pdhg **out);
 void nk_pdhg_destroy(nk_pdhg *h);
 
+/* Pointer arguments of the entries below are required unless their comment
+ * says a null one is skipped; a null required pointer or handle returns
+ * NK_ERR_INVALID. */
+
 /* IterationBackend::advance(count, tau, sigma) -- src/internal.hpp:105,
  * src/cuda.cu:816-866.  Runs `count` PDHG trials with base steps tau, sigma;
  * *accepted receives the accepted progress.  Like the reference CUDA backend it
@@ -90,7 +94,8 @@ nk_status nk_pdhg_monitor(nk_pdhg *h, double *out);
 
 /* IterationBackend::candidates(x, y, xa, ya) -- src/internal.hpp:117-118,
  * src/cuda.cu:867-891: copies the current and averaged iterates to the host
- * arrays (n, m, n, m entries) and rebases the resident A*x. */
+ * arrays (n, m, n, m entries) and rebases the resident A*x.  A null array is
+ * skipped. */
 nk_status nk_pdhg_candidates(nk_pdhg *h, double *x, double *y, double *xa, double *ya);
 
 /* IterationBackend::reset_candidate(average) -- src/internal.hpp:120-122,
@@ -126,7 +131,8 @@ nk_status nk_pdhg_time_spmv(nk_pdhg *h, int which, int reps, double *ms);
 /* The CUDA stream (cudaStream_t) every kernel and copy of this handle runs on,
  * for callers that time the engine with CUDA events. */
 nk_status nk_pdhg_stream(nk_pdhg *h, void **stream);
-/* Row schedule chosen for A and A^T: sub-warp width, long-row threshold, items. */
+/* Row schedule chosen for A and A^T: sub-warp width, long-row threshold, items.
+ * Null outputs are skipped. */
 nk_status nk_pdhg_schedule_info(nk_pdhg *h, int *a_width, int64_t *a_long, int *at_width,
                                 int64_t *at_long, int *a_items, int *at_items);
 
@@ -386,6 +392,8 @@ nk_status nk_linear_solve(const nk_csr *K, const double *rhs, int fp32_matrix, i
 
 int nk_cuda_available(void);
 nk_status nk_cuda_description(char *buffer, int length);
+/* Whether a CUDA device is present, and its free and total memory in bytes
+ * (0 without a device).  Null outputs are skipped. */
 nk_status nk_hardware_info(int *available, double *free_bytes, double *total_bytes);
 
 const char *nk_last_error(void);

@@ -1400,6 +1400,15 @@ HostModel host_model(const nk_model *model) {
 
 using nk::guard;
 
+namespace {
+// A required pointer argument that is null is an argument error reported as
+// NK_ERR_INVALID, never a host crash.
+void need(const void *p, const char *what) {
+    if (!p)
+        throw nk::Error(NK_ERR_INVALID, std::string("null ") + what);
+}
+} // namespace
+
 struct nk_pdhg {
     nk::Engine *e;
 };
@@ -1440,18 +1449,21 @@ nk_status nk_pdhg_advance(nk_pdhg *h, int count, double tau, double sigma, int *
 nk_status nk_pdhg_rejected_steps(nk_pdhg *h, int64_t *out) {
     return guard([&] {
         NK_HANDLE
+        need(out, "output");
         *out = h->e->rejected;
     });
 }
 nk_status nk_pdhg_restart_requested(nk_pdhg *h, int *out) {
     return guard([&] {
         NK_HANDLE
+        need(out, "output");
         *out = h->e->request_restart ? 1 : 0;
     });
 }
 nk_status nk_pdhg_monitor(nk_pdhg *h, double *out) {
     return guard([&] {
         NK_HANDLE
+        need(out, "output");
         *out = h->e->monitor();
     });
 }
@@ -1533,12 +1545,17 @@ nk_status nk_pdhg_reset_candidate(nk_pdhg *h, int average) {
 nk_status nk_pdhg_reset(nk_pdhg *h, const double *x, const double *y) {
     return guard([&] {
         NK_HANDLE
+        if (h->e->n)
+            need(x, "x");
+        if (h->e->m)
+            need(y, "y");
         h->e->reset(x, y);
     });
 }
 nk_status nk_pdhg_snapshot_layout(nk_pdhg *h, int *parts, int64_t *sizes) {
     return guard([&] {
         NK_HANDLE
+        need(parts, "part count");
         auto L = h->e->layout();
         *parts = int(L.size());
         if (sizes)
@@ -1549,12 +1566,15 @@ nk_status nk_pdhg_snapshot_layout(nk_pdhg *h, int *parts, int64_t *sizes) {
 nk_status nk_pdhg_snapshot(nk_pdhg *h, double *out) {
     return guard([&] {
         NK_HANDLE
+        need(out, "snapshot buffer");
         h->e->snapshot(out);
     });
 }
 nk_status nk_pdhg_restore(nk_pdhg *h, const double *in, const int64_t *sizes, int parts) {
     return guard([&] {
         NK_HANDLE
+        need(in, "snapshot");
+        need(sizes, "part sizes");
         h->e->restore(in, sizes, parts);
     });
 }
@@ -1571,6 +1591,8 @@ nk_status nk_pdhg_profile(nk_pdhg *h, int count, double tau, double sigma, doubl
                           double *ms_dual) {
     return guard([&] {
         NK_HANDLE
+        need(ms_primal, "output");
+        need(ms_dual, "output");
         h->e->profile(count, tau, sigma, ms_primal, ms_dual);
     });
 }
@@ -1579,12 +1601,14 @@ nk_status nk_pdhg_time_spmv(nk_pdhg *h, int which, int reps, double *ms) {
         NK_HANDLE
         if (which != 0 && which != 1)
             throw nk::Error(NK_ERR_INVALID, "which must be 0 (A) or 1 (A^T)");
+        need(ms, "output");
         *ms = h->e->time_spmv(which, reps);
     });
 }
 nk_status nk_pdhg_stream(nk_pdhg *h, void **stream) {
     return guard([&] {
         NK_HANDLE
+        need(stream, "output");
         *stream = reinterpret_cast<void *>(h->e->stream);
     });
 }
@@ -1592,13 +1616,18 @@ nk_status nk_pdhg_schedule_info(nk_pdhg *h, int *a_width, int64_t *a_long, int *
                                 int64_t *at_long, int *a_items, int *at_items) {
     return guard([&] {
         NK_HANDLE
-        // SELL-32: one lane per row; reported: lanes per row, split length, chunks
-        *a_width = 1;
-        *a_long = NK_SPLIT;
-        *at_width = 1;
-        *at_long = NK_SPLIT;
-        *a_items = int((h->e->A.nv + 31) / 32);
-        *at_items = int((h->e->At.nv + 31) / 32);
+        // SELL-32: one lane per row; reported: lanes per row, split length,
+        // chunks.  Null outputs are skipped.
+        auto put = [](auto *dst, auto v) {
+            if (dst)
+                *dst = v;
+        };
+        put(a_width, 1);
+        put(a_long, int64_t(NK_SPLIT));
+        put(at_width, 1);
+        put(at_long, int64_t(NK_SPLIT));
+        put(a_items, int((h->e->A.nv + 31) / 32));
+        put(at_items, int((h->e->At.nv + 31) / 32));
     });
 }
 int nk_cuda_available(void) {
@@ -1702,13 +1731,16 @@ nk_status nk_linear_solve(const nk_csr *K, const double *rhs, int fp32_matrix, i
 
 nk_status nk_hardware_info(int *available, double *free_bytes, double *total_bytes) {
     return guard([&] {
-        *available = nk_cuda_available();
-        *free_bytes = *total_bytes = 0;
+        const int present = nk_cuda_available();
         size_t f = 0, t = 0;
-        if (*available && cudaMemGetInfo(&f, &t) == cudaSuccess) {
+        if (present && cudaMemGetInfo(&f, &t) != cudaSuccess)
+            f = t = 0;
+        if (available)
+            *available = present;
+        if (free_bytes)
             *free_bytes = double(f);
+        if (total_bytes)
             *total_bytes = double(t);
-        }
     });
 }
 

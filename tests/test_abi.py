@@ -110,3 +110,35 @@ def test_side_entries_report_a_missing_device():
     with pytest.raises(engine.EngineError) as e:
         engine.propagate_bounds(m, np.zeros(m.n, dtype=np.int32), m.lb, m.ub)
     assert e.value.status == "NO_DEVICE"
+
+
+def test_null_pointers_are_argument_errors():
+    """A null handle or a null required pointer is answered with NK_ERR_INVALID
+    and a message, never a host crash; destroy, free and defaults accept null;
+    the info entries skip null outputs.  Runs through the C ABI with no GPU."""
+    L = C.CDLL(str(engine.LIB_PATH))
+    L.nk_last_error.restype = C.c_char_p
+    INVALID, P, d = 1, C.c_void_p(), C.c_double
+    assert L.nk_pdhg_advance(P, 1, d(1.0), d(1.0), P) == INVALID
+    assert L.nk_last_error() == b"null engine handle"
+    for name in ("nk_pdhg_rejected_steps", "nk_pdhg_restart_requested", "nk_pdhg_monitor",
+                 "nk_pdhg_snapshot", "nk_pdhg_stream"):
+        assert getattr(L, name)(P, P) == INVALID, name
+    assert L.nk_pdhg_candidates(P, P, P, P, P) == INVALID
+    assert L.nk_pdhg_reset(P, P, P) == INVALID
+    assert L.nk_pdhg_restore(P, P, P, 10) == INVALID
+    assert L.nk_pdhg_create(P, P, P, P, P, P, P, P, P, P, P, P) == INVALID
+    assert L.nk_prepare(P, 1, 0, 5, P) == INVALID
+    assert L.nk_solve(P, P, P, P, P) == INVALID
+    assert L.nk_verify(P, P, P, 0, P) == INVALID
+    assert L.nk_batch_create(P, P) == INVALID
+    assert L.nk_batch_estimate(P, P) == INVALID
+    assert L.nk_batch_step(P, 1, P, 0, P) == INVALID
+    assert L.nk_batch_result(P, C.c_int64(0), P, P, P) == INVALID
+    assert L.nk_cuda_description(P, 0) == INVALID
+    for name in ("nk_pdhg_destroy", "nk_batch_destroy", "nk_prepared_free",
+                 "nk_batch_item_free", "nk_solve_defaults", "nk_batch_defaults"):
+        getattr(L, name)(P)
+    assert L.nk_hardware_info(P, P, P) == 0
+    total = d(-1.0)
+    assert L.nk_hardware_info(P, P, C.byref(total)) == 0 and total.value >= 0
