@@ -165,8 +165,8 @@ def build_model(args):
 
 def workload_name(args):
     f = 0.1 if args.small else args.scale
-    return ("config2_power_law_lp_m1e6_n2e6_nnz2e7" if f == 1.0 else
-            f"config2_shape_scaled_{f:g}")
+    return ("power_law_lp_m1e6_n2e6_nnz2e7" if f == 1.0 else
+            f"power_law_lp_scaled_{f:g}")
 
 
 # ---------------------------------------------------------------- CPU arm
@@ -296,12 +296,74 @@ def reference_arm(args, world, rank):
     print(json.dumps(line))
 
 
+# ---------------------------------------------------------------- ingestion
+def write_native_json(model, path):
+    """The reference's native JSON model (read_json, src/io.cpp:84-142) of a
+    minimisation LP, streamed row by row; infinite bounds as "inf" / "-inf"."""
+    def num(v):
+        v = float(v)
+        return repr(v) if math.isfinite(v) else ('"inf"' if v > 0 else '"-inf"')
+
+    with open(path, "w") as f:
+        f.write('{"name":"%s","sense":"min","variables":[' % model.name)
+        f.write(",".join('{"name":"x%d","lb":%s,"ub":%s}' % (j, num(lo), num(hi))
+                         for j, (lo, hi) in enumerate(zip(model.lb, model.ub))))
+        f.write('],"constraints":[')
+        for i in range(model.m):
+            s, e = int(model.ptr[i]), int(model.ptr[i + 1])
+            coef = ",".join('"x%d":%r' % (j, v) for j, v in
+                            zip(model.idx[s:e].tolist(), model.val[s:e].tolist()))
+            f.write('%s{"name":"r%d","lb":%s,"ub":%s,"coefficients":{%s}}'
+                    % ("," if i else "", i, num(model.rl[i]), num(model.ru[i]), coef))
+        f.write('],"objective":{"linear":[%s],"offset":%r}}'
+                % (",".join(map(repr, model.c.tolist())), float(model.offset)))
+
+
+def ingest_section(args):
+    """Model ingestion of the power-law LP: written to a model file and loaded
+    back (memory map plus the header, size, checksum and CSR checks), best of
+    three loads on a warm page cache.  With --impl reference also the
+    reference's own read_model (src/io.cpp:800-814) on the same model's native
+    JSON, and whether it built exactly the arrays the model file holds."""
+    from niryukti_b200 import modelfile
+    model = build_model(args)
+    out = {"workload": workload_name(args), "m": model.m, "n": model.n, "nnz": model.nnz}
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "model.nkm")
+        t = time.perf_counter()
+        modelfile.save(model, path)
+        out["save_s"] = time.perf_counter() - t
+        out["file_mb"] = os.path.getsize(path) / 1e6
+        loads = []
+        for _ in range(3):
+            t = time.perf_counter()
+            back = modelfile.load(path)
+            loads.append(time.perf_counter() - t)
+            del back
+        out["load_s"] = min(loads)
+        if args.impl == "reference":
+            from oracle import oracle as orc
+            jpath = os.path.join(d, "model.json")
+            t = time.perf_counter()
+            write_native_json(model, jpath)
+            out["json_write_s"] = time.perf_counter() - t
+            out["json_mb"] = os.path.getsize(jpath) / 1e6
+            t = time.perf_counter()
+            ref = orc.Reference().read_model(jpath)
+            out["reference_read_s"] = time.perf_counter() - t
+            back = modelfile.load(path)
+            out["identical"] = all(np.array_equal(getattr(ref, f), getattr(back, f))
+                                   for f in ("ptr", "idx", "val", "c", "q", "lb", "ub", "rl",
+                                             "ru"))
+    print(json.dumps({"ingest": out}))
+
+
 # ---------------------------------------------------------------- solves
 def solve_models(args):
     from niryukti_b200 import synth
     c1 = synth.random_lp(m=2000, n=5000, per_col=5, seed=1)
     c2 = build_model(args)
-    return {"config1_lp_m2000_n5000": c1, workload_name(args): c2}
+    return {"random_lp_m2000_n5000": c1, workload_name(args): c2}
 
 
 def reference_solve(model, budget, threads, iteration_limit=10**9):
@@ -341,7 +403,7 @@ def reference_solve(model, budget, threads, iteration_limit=10**9):
 def solve_child(args):
     out = {}
     for name, model in solve_models(args).items():
-        budget = args.cpu_solve_seconds if "config2" in name else 300.0
+        budget = args.cpu_solve_seconds if name.startswith("power_law_lp") else 300.0
         out[name] = reference_solve(model, budget, args.cpu_threads)
     print(json.dumps(out))
 
@@ -353,7 +415,7 @@ def solve_section(args):
     from niryukti_b200 import solver
     res = {}
     for name, model in solve_models(args).items():
-        budget = args.solve_seconds if "config2" in name else 300.0
+        budget = args.solve_seconds if name.startswith("power_law_lp") else 300.0
         r = solver.solve(model, tol=1e-6, time_limit=budget, iteration_limit=10**9,
                          matrix_precision="fp64")
         res[name] = {"gpu": {k: r[k] for k in (
@@ -363,7 +425,7 @@ def solve_section(args):
         res[name]["gpu"]["budget_s"] = budget
         # FP32 matrices first, then the closing FP64 refinement from the best
         # reduced-precision point; accuracy of both against the FP64 solve
-        precs = ("mixed", "fp32") if "config2" not in name else ("mixed",)
+        precs = ("mixed",) if name.startswith("power_law_lp") else ("mixed", "fp32")
         for prec in precs if not args.no_forms else ():
             q = solver.solve(model, tol=1e-6, time_limit=budget, iteration_limit=10**9,
                              matrix_precision=prec, refine=True)
@@ -453,7 +515,7 @@ def batch_section(args):
     # instance times the instance count estimates the one-by-one total
     total_nnz = sum(m.nnz for m in models)
     plain_s = sum(p["seconds"] for p in plain) / len(plain) * len(models)
-    out = {"workload": f"config4_{len(models)}_uneven_lp_qp_m500_{args.batch_m_hi}",
+    out = {"workload": f"uneven_lp_qp_{len(models)}_m500_{args.batch_m_hi}",
            "instances": len(models), "qp": sum(1 for m in models if m.is_qp()),
            "total_nnz": total_nnz, "precision": args.batch_precision, "tol": 1e-6,
            "statuses": statuses, "worst_certified_kkt": worst,
@@ -507,7 +569,7 @@ def batch_throughput(args):
         kp, kd = eng.kernel_times()
         info = eng.info()
     per = ms / max(1, args.batch_trials)
-    return {"workload": f"config4_{len(models)}_uneven_lp_qp", "precision": args.batch_precision,
+    return {"workload": f"uneven_lp_qp_{len(models)}", "precision": args.batch_precision,
             "trials": args.batch_trials, "ms_per_trial": per,
             "spmv_bytes_per_trial": bts, "spmv_GBps": bts / per / 1e6,
             "tuned_kernel_ms": {"batch_primal": kp, "batch_dual": kd},
@@ -591,7 +653,7 @@ def serve_section(args):
             lat.append(end - a)
             done += 1
     plain = summary(lat, done, horizon)
-    return {"workload": f"config5_poisson_{args.serve_rate:g}_per_s_{args.serve_seconds:g}s_"
+    return {"workload": f"poisson_{args.serve_rate:g}_per_s_{args.serve_seconds:g}s_"
                         f"m500_200000", "pool": len(pool), "window_s": horizon,
             "served_continuous_batching": served, "plain_fp64_one_at_a_time": plain}
 
@@ -644,7 +706,7 @@ def time_form(model, precision, steps, warmup, profile_trials):
         torch.cuda.synchronize()
 
 
-def config3_section(args):
+def block_angular_section(args):
     """The block-angular planning LP (64 blocks of 20,000 x 40,000
     with 6 nonzeros per column, 2,000 linking rows over 5% of all columns
     each), iteration rate in FP64 and with FP32 matrices."""
@@ -652,14 +714,14 @@ def config3_section(args):
     from niryukti_b200 import synth
     torch.cuda.set_device(0)
     t0 = time.perf_counter()
-    model = synth.block_angular_lp(blocks=args.config3_blocks)
+    model = synth.block_angular_lp(blocks=args.block_angular_blocks)
     gen_s = time.perf_counter() - t0
     peaks = {}
     pk = ROOT / "MEASURED_PEAKS.json"
     if pk.exists():
         peaks = json.loads(pk.read_text())
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    out = {"workload": f"config3_block_angular_b{args.config3_blocks}_20000x40000_link2000",
+    out = {"workload": f"block_angular_b{args.block_angular_blocks}_20000x40000_link2000",
            "m": model.m, "n": model.n, "nnz": model.nnz, "generate_s": gen_s,
            "peak_GBps": peak, "forms": {}}
     for prec in ("fp64", "mixed"):
@@ -725,7 +787,7 @@ def engine_arm(args, world, rank, local):
     traffic, traffic_source = args.traffic, "--traffic" if args.traffic else None
     if traffic is None and args.precision == "fp64" and not args.small and args.scale == 1.0:
         # DRAM bytes per launch from the ncu capture of the power-law LP at half
-        # size (profiles/fused_pdhg_kernels_config2_scaled_half.md: read + write),
+        # size (profiles/fused_pdhg_kernels_power_law_lp_half_scale.md: read + write),
         # scaled by 2: every unit (nonzeros, rows, columns) doubles
         traffic = {"primal_kernel": 2 * 181.32e6, "dual_kernel": 2 * 166.24e6}[top]
         traffic_source = "ncu dram__bytes_read.sum + dram__bytes_write.sum at scale 0.5, x2"
@@ -859,9 +921,12 @@ def main():
                     help="smallest sampled instances also solved by the reference on the CPU")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the FP32-matrix forms of the power-law LP iteration rate")
-    ap.add_argument("--config3", action="store_true",
+    ap.add_argument("--block-angular", action="store_true",
                     help="print only the block-angular LP iteration-rate section")
-    ap.add_argument("--config3-blocks", type=int, default=64)
+    ap.add_argument("--block-angular-blocks", type=int, default=64)
+    ap.add_argument("--ingest", action="store_true",
+                    help="time model-file ingestion (and, with --impl reference, the "
+                         "reference's JSON reader on the same model); CPU only")
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per launch of the top kernel from an ncu capture")
     args = ap.parse_args()
@@ -880,9 +945,11 @@ def main():
     if args.serve:
         print(json.dumps({"serve": serve_section(args)}))
         return
-    if args.config3:
-        print(json.dumps({"config3": config3_section(args)}))
+    if args.block_angular:
+        print(json.dumps({"block_angular": block_angular_section(args)}))
         return
+    if args.ingest:
+        return ingest_section(args)
     world, rank, local = dist_setup()
     if args.impl == "reference":
         return reference_arm(args, world, rank)

@@ -390,6 +390,29 @@ nk_status nk_propagate_bounds(const nk_csr *A, const int *integer, const double 
 nk_status nk_linear_solve(const nk_csr *K, const double *rhs, int fp32_matrix, int precondition,
                           double time_limit, double *x, int *converged, int *timed_out);
 
+/* ------------------------------------------------------------------ model file
+ * Binary model file (no reference counterpart): the arrays of an nk_model
+ * stored raw, so that a large instance loads by mapping a file instead of the
+ * text parse the reference does for its JSON and MPS formats
+ * (src/io.cpp:84-139,299,800; its Python session passes every model through a
+ * temporary JSON file, python/vantage/native.py:26-31).  The layout is given
+ * at the top of niryukti_b200/csrc/nk_modelfile.cpp. */
+typedef struct nk_model_file nk_model_file;
+/* Writes `model` to `path` (through "<path>.tmp" and a rename).  A model
+ * without q stores zeros; Q is stored when it has entries.  `maximise` != 0
+ * records that the source objective was a maximisation whose minimisation
+ * form `model` holds (the reference's Model::sense = -1). */
+nk_status nk_model_write(const char *path, const nk_model *model, int maximise);
+/* Maps `path` read-only and points *model into the mapping after checking the
+ * header, the file size, the checksum and the CSR structure of A and Q;
+ * *maximise (may be NULL) receives the recorded sense.  The pointers stay
+ * valid until nk_model_close(*file). */
+nk_status nk_model_open(const char *path, nk_model_file **file, nk_model *model, int *maximise);
+void nk_model_close(nk_model_file *file);
+/* The checks of nk_model_open on a file image already in memory (8-byte
+ * aligned, `bytes` long); *model points into the image. */
+nk_status nk_model_view(const void *image, int64_t bytes, nk_model *model, int *maximise);
+
 int nk_cuda_available(void);
 nk_status nk_cuda_description(char *buffer, int length);
 /* Whether a CUDA device is present, and its free and total memory in bytes

@@ -20,7 +20,7 @@ HERE = pathlib.Path(__file__).resolve().parent
 ROOT = HERE.parent
 CSRC = HERE / "csrc"
 OUT = HERE / "libnkpdhg.so"
-SOURCES = ["nk_engine.cu"]
+SOURCES = ["nk_engine.cu", "nk_modelfile.cpp"]  # nvcc: CUDA and the host code that shares its errors
 HOST_SOURCES = ["nk_prepare.cpp"]  # plain C++: presolve, scaling, verifier
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

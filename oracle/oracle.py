@@ -314,6 +314,43 @@ class Reference:
         L.ref_batch_relaxations.argtypes = [C.c_void_p, C.c_int, _D, _D, _D, _D, C.c_char_p, _D,
                                             C.POINTER(C.c_int), _D, _D]
         L.ref_linear_solve.argtypes = [C.c_int64, _I, _I, _D, _D, C.c_int, C.c_double, _D]
+        L.ref_model_read.restype = C.c_void_p
+        L.ref_model_read.argtypes = [C.c_char_p]
+        L.ref_model_dims.argtypes = [C.c_void_p, _I]
+        L.ref_model_arrays.argtypes = [C.c_void_p, _D, _D, _D, _D, _D, _D, _D, _I, _I, _D]
+
+    def read_model(self, path):
+        """The model the reference's read_model (src/io.cpp:800-814) builds from
+        a JSON, MPS, LP or QPLIB file, as a synth.Model of its continuous arrays
+        (canonical CSR of A and Q, c, q, bounds, offset)."""
+        from niryukti_b200 import synth
+        h = self.lib.ref_model_read(str(path).encode())
+        if not h:
+            raise RuntimeError(self.error())
+        try:
+            dims = np.zeros(5, dtype=np.int64)
+            self.lib.ref_model_dims(h, _i(dims))
+            m, n, nnz, qnnz, integer = (int(v) for v in dims)
+            if integer:
+                raise ValueError(f"{integer} integer columns: not a continuous model")
+            ptr = np.zeros(m + 1, dtype=np.int64)
+            idx = np.zeros(nnz, dtype=np.int64)
+            val = np.zeros(nnz)
+            self.lib.ref_model_csr(h, _i(ptr), _i(idx), _d(val))
+            vec = {k: np.zeros(n) for k in ("c", "q", "lb", "ub")}
+            vec.update({k: np.zeros(m) for k in ("rl", "ru")})
+            offset = np.zeros(1)
+            qptr = np.zeros(n + 1, dtype=np.int64)
+            qidx = np.zeros(qnnz, dtype=np.int64)
+            qval = np.zeros(qnnz)
+            self.lib.ref_model_arrays(h, *(_d(vec[k]) for k in ("c", "q", "lb", "ub", "rl", "ru")),
+                                      _d(offset), _i(qptr), _i(qidx), _d(qval))
+        finally:
+            self.lib.ref_model_free(h)
+        q = (qptr, qidx, qval) if qnnz else (None, None, None)
+        return synth.Model(m=m, n=n, ptr=ptr, idx=idx, val=val, c=vec["c"], q=vec["q"],
+                           lb=vec["lb"], ub=vec["ub"], rl=vec["rl"], ru=vec["ru"], qptr=q[0],
+                           qidx=q[1], qval=q[2], offset=float(offset[0]))
 
     def linear_solve(self, ptr, idx, val, rhs, fp32_matrix=False, tolerance=1e-7):
         """cuda_linear_solve(K, rhs, Options(), fp32_matrix, tolerance)."""

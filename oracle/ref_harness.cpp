@@ -160,6 +160,55 @@ void ref_model_multiply(ref_model *r, const double *x, double *out) {
 }
 double ref_model_quadratic_norm_bound(ref_model *r) { return r->m.quadratic_norm_bound(); }
 
+// The reference's own model reader (read_model, src/io.cpp:800-814: JSON,
+// MPS, LP or QPLIB by file extension).
+ref_model *ref_model_read(const char *path) {
+    try {
+        auto *r = new ref_model;
+        r->m = read_model(path);
+        return r;
+    } catch (const std::exception &e) {
+        set_error(e.what());
+        return nullptr;
+    }
+}
+// {m, n, nnz, qnnz, integer columns} of a model.
+void ref_model_dims(ref_model *r, int64_t *dims) {
+    const Model &M = r->m;
+    dims[0] = int64_t(M.rl.size());
+    dims[1] = int64_t(M.c.size());
+    dims[2] = int64_t(M.A.value.size());
+    dims[3] = M.Q.ptr.empty() ? 0 : int64_t(M.Q.value.size());
+    int64_t integer = 0;
+    for (auto t : M.types)
+        integer += t != VarType::Continuous;
+    dims[4] = integer;
+}
+// The continuous arrays of a model; q is zero when the model has none, and
+// Q's arrays are written only when it has entries.
+void ref_model_arrays(ref_model *r, double *c, double *q, double *lb, double *ub, double *rl,
+                      double *ru, double *offset, int64_t *qptr, int64_t *qidx, double *qval) {
+    const Model &M = r->m;
+    auto put = [](double *dst, const std::vector<double> &v) {
+        std::memcpy(dst, v.data(), v.size() * sizeof(double));
+    };
+    put(c, M.c);
+    if (M.q.size() == M.c.size())
+        put(q, M.q);
+    else
+        std::fill(q, q + M.c.size(), 0.0);
+    put(lb, M.lb);
+    put(ub, M.ub);
+    put(rl, M.rl);
+    put(ru, M.ru);
+    *offset = M.offset;
+    if (!M.Q.ptr.empty() && !M.Q.value.empty()) {
+        std::memcpy(qptr, M.Q.ptr.data(), M.Q.ptr.size() * sizeof(int64_t));
+        std::memcpy(qidx, M.Q.index.data(), M.Q.index.size() * sizeof(int64_t));
+        put(qval, M.Q.value);
+    }
+}
+
 // stats: [objective, primal, dual, gap, kkt, primal_abs, dual_abs, complementarity,
 //         lower_bound, finite, iterations, restarts, rejected_steps, seconds,
 //         iteration_seconds, verification_seconds, preprocess_seconds, weight_updates,
