@@ -142,3 +142,21 @@ def test_null_pointers_are_argument_errors():
     assert L.nk_hardware_info(P, P, P) == 0
     total = d(-1.0)
     assert L.nk_hardware_info(P, P, C.byref(total)) == 0 and total.value >= 0
+
+
+def test_plain_c_caller(tmp_path):
+    """include/nk_pdhg.h compiles as strict C99 and a C program linked against
+    the library runs its host-only entries (tests/c/abi_host.c)."""
+    exe = tmp_path / "abi_host"
+    lib_dir = engine.LIB_PATH.parent
+    subprocess.check_call(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic",
+                           f"-I{ROOT / 'include'}", str(ROOT / "tests" / "c" / "abi_host.c"),
+                           f"-L{lib_dir}", "-lnkpdhg", f"-Wl,-rpath,{lib_dir}", "-lm",
+                           "-o", str(exe)])
+    out = subprocess.run([str(exe), str(tmp_path / "lp.nkm")], capture_output=True, text=True,
+                         timeout=120)
+    assert out.returncode == 0, out.stderr
+    words = out.stdout.split()
+    assert words[:4] == ["rows", "2", "cols", "2"]
+    assert float(words[5]) == pytest.approx(-2.8, rel=1e-12)
+    assert float(words[7]) < 1e-12
