@@ -314,16 +314,20 @@ class Reference:
         L.ref_batch_relaxations.argtypes = [C.c_void_p, C.c_int, _D, _D, _D, _D, C.c_char_p, _D,
                                             C.POINTER(C.c_int), _D, _D]
         L.ref_linear_solve.argtypes = [C.c_int64, _I, _I, _D, _D, C.c_int, C.c_double, _D]
-        L.ref_model_read.restype = C.c_void_p
-        L.ref_model_read.argtypes = [C.c_char_p]
-        L.ref_model_dims.argtypes = [C.c_void_p, _I]
-        L.ref_model_arrays.argtypes = [C.c_void_p, _D, _D, _D, _D, _D, _D, _D, _I, _I, _D]
+        if hasattr(L, "ref_model_read"):  # absent from builds older than the reader
+            L.ref_model_read.restype = C.c_void_p
+            L.ref_model_read.argtypes = [C.c_char_p]
+            L.ref_model_dims.argtypes = [C.c_void_p, _I]
+            L.ref_model_arrays.argtypes = [C.c_void_p, _D, _D, _D, _D, _D, _D, _D, _I, _I, _D]
 
     def read_model(self, path):
         """The model the reference's read_model (src/io.cpp:800-814) builds from
         a JSON, MPS, LP or QPLIB file, as a synth.Model of its continuous arrays
         (canonical CSR of A and Q, c, q, bounds, offset)."""
         from niryukti_b200 import synth
+        if not hasattr(self.lib, "ref_model_read"):
+            raise RuntimeError("this reference build predates ref_model_read; rebuild "
+                               "(make -C oracle ref bridge)")
         h = self.lib.ref_model_read(str(path).encode())
         if not h:
             raise RuntimeError(self.error())
