@@ -1345,8 +1345,8 @@ Engine *create_engine(const nk_csr *Ah, const nk_csr *Qh, const double *hc, cons
 #include "nk_newton.cuh"
 
 namespace nk {
-// Copies a caller model (C ABI) into the host representation, after the
-// structural checks of Model::validate for the continuous part.
+// Copies a caller model (C ABI) into the host representation, with the checks
+// of Model::validate for the continuous part (src/model.cpp:74-123).
 HostModel host_model(const nk_model *model) {
     if (!model)
         throw Error(NK_ERR_INVALID, "null model");
@@ -1394,6 +1394,11 @@ HostModel host_model(const nk_model *model) {
         if (std::isnan(l) || std::isnan(u) || l == kInf || u == -kInf || l > u)
             throw Error(NK_ERR_INVALID, "Invalid row bounds");
     }
+    // coefficients and indices of A and Q; the reference's further convexity
+    // certificate for a Q that is not diagonally dominant (a sparse LU above
+    // 256 columns, a dense elimination below, src/model.cpp:143-252) is not
+    // repeated: a non-convex Q is the caller's error
+    validate_entries(hm);
     return hm;
 }
 } // namespace nk

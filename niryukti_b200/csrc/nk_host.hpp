@@ -66,6 +66,12 @@ struct HostSerialScope { // serial host loops on this thread until the scope end
 
 Csr build_csr(int64_t rows, int64_t cols, std::vector<Entry> e);
 Csr transpose(const Csr &a);
+// The entry checks of Model::validate (src/model.cpp:107-123) for a model whose
+// CSR offsets are already valid: every coefficient of A and Q finite and every
+// column index inside [0, cols); Q's columns strictly increase within a row and
+// Q equals its transpose exactly.  Throws std::runtime_error with the
+// reference's message.
+void validate_entries(const HostModel &m);
 Prepared prepare(const HostModel &src, const PrepareOptions &o);
 
 // Verifier over one original model; keeps A^T like the reference's Verifier.

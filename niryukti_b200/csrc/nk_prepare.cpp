@@ -239,6 +239,32 @@ Csr build_csr(int64_t rows, int64_t cols, std::vector<Entry> e) {
 // a sequential row sweep).  Large matrices are swept by contiguous row blocks
 // in parallel: block b places its entries of column j after those of blocks
 // before it, so the result is the sequential one entry for entry.
+void validate_entries(const HostModel &m) {
+    const int64_t n = int64_t(m.c.size()), nnz = int64_t(m.A.value.size());
+    int bad = 0;
+#pragma omp parallel for reduction(max : bad) if (nnz > 200000 && !g_host_serial)
+    for (int64_t k = 0; k < nnz; ++k)
+        if (m.A.index[size_t(k)] < 0 || m.A.index[size_t(k)] >= n ||
+            !std::isfinite(m.A.value[size_t(k)]))
+            bad = 1;
+    if (bad)
+        throw std::runtime_error("Invalid matrix coefficient/index");
+    if (m.Q.value.empty())
+        return;
+    for (int64_t i = 0; i < m.Q.rows; ++i) {
+        int64_t previous = -1;
+        for (auto k = m.Q.ptr[size_t(i)]; k < m.Q.ptr[size_t(i + 1)]; ++k) {
+            const int64_t j = m.Q.index[size_t(k)];
+            if (j <= previous || j >= n || !std::isfinite(m.Q.value[size_t(k)]))
+                throw std::runtime_error("Invalid quadratic coefficient/index");
+            previous = j;
+        }
+    }
+    const Csr t = transpose(m.Q);
+    if (t.ptr != m.Q.ptr || t.index != m.Q.index || t.value != m.Q.value)
+        throw std::runtime_error("Quadratic matrix must be exactly symmetric");
+}
+
 Csr transpose(const Csr &a) {
     Csr t;
     t.rows = a.cols;
@@ -374,6 +400,7 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
     std::vector<char> verdict(size_t(mrows), KEEP), dupcand(size_t(mrows), 0);
     std::vector<double> row_l(static_cast<size_t>(mrows)), row_u(static_cast<size_t>(mrows));
     std::vector<uint64_t> key_hash(size_t(mrows), 0);
+    std::vector<int64_t> kept_in_row(size_t(mrows), 0); // entries in kept columns
     const long double eps = std::numeric_limits<long double>::epsilon();
 #pragma omp parallel for schedule(dynamic, 1024) if (src.A.value.size() > 200000 && !g_host_serial)
     for (int64_t i = 0; i < mrows; i++) {
@@ -389,6 +416,7 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
             } else
                 count++;
         }
+        kept_in_row[size_t(i)] = count;
         double l = src.rl[i] - double(shift), u = src.ru[i] - double(shift);
         row_l[size_t(i)] = l;
         row_u[size_t(i)] = u;
@@ -403,10 +431,20 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
                 continue;
             }
         }
+        // Activity bounds.  A column with an infinite bound makes amin or amax
+        // infinite or NaN (for either sign of v), an infinite or NaN sum stays
+        // so, and the verdicts below use the bounds only when both are finite:
+        // such a row's verdict is settled at that column, so the sum stops
+        // there.  (Carrying long double infinities through the rest of every
+        // such row took most of prepare's time on models with free columns.)
         long double amin = 0, amax = 0, magnitude = 0;
         for (auto k = b; k < en; k++) {
             auto j = src.A.index[size_t(k)];
             double v = src.A.value[size_t(k)];
+            if (!std::isfinite(src.lb[j]) || !std::isfinite(src.ub[j])) {
+                amin = -std::numeric_limits<long double>::infinity();
+                break;
+            }
             amin += (long double)v * (v > 0 ? src.lb[j] : src.ub[j]);
             amax += (long double)v * (v > 0 ? src.ub[j] : src.lb[j]);
             magnitude += std::abs((long double)v * (v > 0 ? src.lb[j] : src.ub[j])) +
@@ -490,8 +528,7 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
         p.upper_rows.push_back(i);
         m.rl.push_back(l);
         m.ru.push_back(u);
-        for (auto k = b; k < en; k++)
-            kept_entries += map[size_t(src.A.index[size_t(k)])] >= 0;
+        kept_entries += size_t(kept_in_row[size_t(i)]);
     }
     // The kept entries.  When every kept row's columns strictly increase (a
     // canonical CSR: the map keeps column order), Sparse::build would only drop

@@ -160,3 +160,36 @@ def test_plain_c_caller(tmp_path):
     assert words[:4] == ["rows", "2", "cols", "2"]
     assert float(words[5]) == pytest.approx(-2.8, rel=1e-12)
     assert float(words[7]) < 1e-12
+
+
+def test_model_entries_are_checked_like_the_reference():
+    """The host entries (nk_prepare, nk_solve, nk_verify, nk_batch_*) refuse the
+    entries Model::validate refuses (src/model.cpp:107-123), before any host
+    array is indexed by them."""
+    from niryukti_b200 import solver
+    from tests.test_oracle import sparse_qp_model
+
+    def refused(model, message):
+        with pytest.raises(engine.EngineError, match=message) as e:
+            solver.prepare(model)
+        assert e.value.status == "INVALID"
+
+    lp = synth.random_lp(m=20, n=40, per_col=2, seed=3)
+    for k, bad in ((5, lp.n), (7, -1)):
+        m = synth.Model(**{**lp.__dict__, "idx": lp.idx.copy()})
+        m.idx[k] = bad
+        refused(m, "Invalid matrix coefficient/index")
+    for bad in (np.nan, np.inf):
+        m = synth.Model(**{**lp.__dict__, "val": lp.val.copy()})
+        m.val[3] = bad
+        refused(m, "Invalid matrix coefficient/index")
+    qp = sparse_qp_model()
+    assert qp.qnnz >= 2
+    m = synth.Model(**{**qp.__dict__, "qval": qp.qval.copy()})
+    off = np.flatnonzero(np.repeat(np.arange(qp.n), np.diff(qp.qptr)) != qp.qidx)[0]
+    m.qval[off] += 1.0  # one off-diagonal entry without its mirror
+    refused(m, "exactly symmetric")
+    m = synth.Model(**{**qp.__dict__, "qval": qp.qval.copy()})
+    m.qval[0] = np.nan
+    refused(m, "Invalid quadratic coefficient/index")
+    solver.prepare(qp)  # the valid model still passes

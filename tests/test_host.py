@@ -110,7 +110,31 @@ def random_presolve_model(seed, m=300, n=700, per_col=4, fixed=40, dups=25, redu
     return from_rows(base.n, rows, c=base.c, lb=lb, ub=ub, rl=rl, ru=ru)
 
 
+def infinite_bounds_model():
+    """Rows whose activity-bound verdict hinges on infinite column bounds: a
+    free or one-sided column first, in the middle or last in a row, with either
+    coefficient sign, keeps a row that its finite columns alone would make
+    redundant; the duplicate of such a row is still merged."""
+    inf = np.inf
+    lb = [0, -inf, 0, 0, 0, -inf, 0, 0, 0]
+    ub = [1, inf, 1, inf, 1, 5, 1, 1, 1]
+    rows = [[(0, 1e-4), (2, 1e-4)],                # finite and redundant: dropped
+            [(1, 1e-4), (2, 1e-4), (4, 1e-4)],     # free column first
+            [(0, 1e-4), (1, -1e-4), (2, 1e-4)],    # free column in the middle
+            [(0, 1e-4), (2, 1e-4), (3, 1e-4)],     # upper bound +inf, last
+            [(0, 1e-4), (3, -1e-4)],               # upper bound +inf, negative coefficient
+            [(4, 1e-4), (5, 1e-4)],                # lower bound -inf
+            [(5, -1e-4), (8, 1e-4)],               # lower bound -inf, negative coefficient
+            [(6, 1.0), (7, 1.0)],                  # finite and binding
+            [(3, 1.0), (8, 1.0)],                  # disjoint-looking, but x3 is unbounded
+            [(1, 1e-4), (2, 1e-4), (4, 1e-4)]]     # duplicate of row 1
+    rl = [-1, -1, -1, -1, -1, -1, -1, 0.5, 5, -0.5]
+    ru = [1, 1, 1, 1, 1, 1, 1, 1.5, 10, 0.5]
+    return from_rows(9, rows, c=[1, 0.5, -1, 1, 0, -0.5, 1, 1, 0], lb=lb, ub=ub, rl=rl, ru=ru)
+
+
 MODELS = {
+    "infinite_bounds": infinite_bounds_model,
     "presolve": presolve_model,
     "presolve_qp": presolve_qp,
     "sparse_qp": sparse_qp_model,
@@ -180,6 +204,12 @@ def test_presolve_rules_fire(reference):
     assert 2 not in kept and 3 not in kept                  # empty-after-substitution, redundant
     r0 = p["rows"].tolist().index(0)
     assert p["lower_rows"][r0] == 1 and p["upper_rows"][r0] == 6
+
+
+def test_infinite_bounds_keep_rows():
+    p = solver.prepare(infinite_bounds_model())
+    assert p["rows"].tolist() == [1, 2, 3, 4, 5, 6, 7, 8]  # row 0 dropped, row 9 merged
+    assert p["lower_rows"][0] == 9 and p["upper_rows"][0] == 9
 
 
 def infeasible_models():
