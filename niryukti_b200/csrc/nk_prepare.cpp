@@ -38,14 +38,22 @@ bool representable(double before, double after) {
 // column's factor sets the column's factor to 1; the sequential loop reaches
 // the same verdict (once a column's factor is 1 every later entry takes it),
 // so the verdicts are gathered per column first and applied after.
+//
+// The column half is scale_columns.  `colmax` / `colmin` (optional) hold, as
+// bit patterns, each column's largest |a| and smallest nonzero |a| of the
+// current values; with them the entry verdicts need no pass over the entries:
+// rounding is monotone and sign-symmetric, so every finite a of a column has a
+// finite a*f iff its largest |a| does, and every nonzero a a nonzero a*f iff its
+// smallest nonzero |a| does (all of A's values are finite, Model::validate).
+void scale_columns(Prepared &p, std::vector<double> col, const uint64_t *colmax,
+                   const uint64_t *colmin);
+
 void extra_scale(Prepared &p, const std::vector<double> &row, std::vector<double> col) {
     HostModel &m = p.model;
     const bool par = m.A.value.size() > 200000 && !g_host_serial;
     // A side whose factors are all 1 changes nothing (x * 1 == x, and every
-    // representability test passes): the Ruiz passes scale rows and columns in
-    // separate calls, so each call skips the other side's loops.
+    // representability test passes), so its loops are skipped.
     const bool rows_one = std::all_of(row.begin(), row.end(), [](double f) { return f == 1; });
-    const bool cols_one = std::all_of(col.begin(), col.end(), [](double f) { return f == 1; });
 #pragma omp parallel for schedule(dynamic, 1024) if (par && !rows_one)
     for (int64_t ii = 0; ii < (rows_one ? 0 : int64_t(row.size())); ii++) {
         const size_t i = size_t(ii);
@@ -62,7 +70,14 @@ void extra_scale(Prepared &p, const std::vector<double> &row, std::vector<double
         for (int64_t k = m.A.ptr[i]; k < m.A.ptr[i + 1]; k++)
             m.A.value[k] *= f;
     }
-    if (cols_one)
+    scale_columns(p, std::move(col), nullptr, nullptr);
+}
+
+void scale_columns(Prepared &p, std::vector<double> col, const uint64_t *colmax,
+                   const uint64_t *colmin) {
+    HostModel &m = p.model;
+    const bool par = m.A.value.size() > 200000 && !g_host_serial;
+    if (std::all_of(col.begin(), col.end(), [](double f) { return f == 1; }))
         return;
 #pragma omp parallel for if (par)
     for (int64_t jj = 0; jj < int64_t(col.size()); jj++) {
@@ -74,13 +89,26 @@ void extra_scale(Prepared &p, const std::vector<double> &row, std::vector<double
             col[j] = 1;
     }
     std::vector<unsigned char> refuse(col.size(), 0);
+    if (colmax && colmin) {
 #pragma omp parallel for if (par)
-    for (int64_t kk = 0; kk < int64_t(m.A.value.size()); kk++) {
-        const size_t k = size_t(kk);
-        auto j = m.A.index[k];
-        if (!representable(m.A.value[k], m.A.value[k] * col[size_t(j)])) {
+        for (int64_t jj = 0; jj < int64_t(col.size()); jj++) {
+            const size_t j = size_t(jj);
+            double hi, lo;
+            std::memcpy(&hi, &colmax[j], 8);
+            std::memcpy(&lo, &colmin[j], 8);
+            const bool any_nonzero = colmin[j] != ~uint64_t(0);
+            if (!std::isfinite(hi * col[j]) || (any_nonzero && lo * col[j] == 0))
+                refuse[j] = 1;
+        }
+    } else {
+#pragma omp parallel for if (par)
+        for (int64_t kk = 0; kk < int64_t(m.A.value.size()); kk++) {
+            const size_t k = size_t(kk);
+            auto j = m.A.index[k];
+            if (!representable(m.A.value[k], m.A.value[k] * col[size_t(j)])) {
 #pragma omp atomic write
-            refuse[size_t(j)] = 1;
+                refuse[size_t(j)] = 1;
+            }
         }
     }
     for (size_t j = 0; j < col.size(); j++)
@@ -108,6 +136,58 @@ void extra_scale(Prepared &p, const std::vector<double> &row, std::vector<double
 #pragma omp parallel for if (par)
     for (int64_t kk = 0; kk < int64_t(m.A.value.size()); kk++)
         m.A.value[size_t(kk)] *= col[size_t(m.A.index[size_t(kk)])];
+}
+
+// One Ruiz pass's row half in one sweep (src/preprocess.cpp:310-319: the row
+// norms, the first extra_scale call, then the column norms): each row's
+// largest |a| gives its factor clamp(1/sqrt(norm), 1e-3, 1e3) (1 for a row
+// without nonzeros), the row is scaled exactly as extra_scale's row loop scales
+// it, and the scaled values update the column extremes scale_columns takes --
+// largest |a| and smallest nonzero |a|, as bit patterns, which order like
+// non-negative values, so the maxima and minima do not depend on the order the
+// rows are taken in.  A row whose factor is 1 is left as it is, which is what
+// multiplying it by 1 does.
+void ruiz_rows(Prepared &p, bool par, std::vector<uint64_t> &colmax,
+               std::vector<uint64_t> &colmin) {
+    HostModel &m = p.model;
+#pragma omp parallel for schedule(dynamic, 1024) if (par)
+    for (int64_t ii = 0; ii < int64_t(m.rl.size()); ++ii) {
+        const size_t i = size_t(ii);
+        const int64_t b = m.A.ptr[i], e = m.A.ptr[i + 1];
+        double norm = 0;
+        for (auto k = b; k < e; ++k)
+            norm = std::max(norm, std::abs(m.A.value[size_t(k)]));
+        const double f = norm > 0 ? std::clamp(1 / std::sqrt(norm), 1e-3, 1e3) : 1.;
+        if (f != 1) {
+            bool safe = representable(p.row_scale[i], p.row_scale[i] * f) &&
+                        representable(m.rl[i], m.rl[i] * f) && representable(m.ru[i], m.ru[i] * f);
+            for (auto k = b; k < e; k++)
+                safe &= representable(m.A.value[size_t(k)], m.A.value[size_t(k)] * f);
+            if (safe) {
+                p.row_scale[i] *= f;
+                m.rl[i] *= f;
+                m.ru[i] *= f;
+                for (auto k = b; k < e; k++)
+                    m.A.value[size_t(k)] *= f;
+            }
+        }
+        for (auto k = b; k < e; ++k) {
+            const double v = std::abs(m.A.value[size_t(k)]);
+            if (v == 0)
+                continue;
+            uint64_t bits;
+            std::memcpy(&bits, &v, 8);
+            const size_t j = size_t(m.A.index[size_t(k)]);
+            uint64_t cur = __atomic_load_n(&colmax[j], __ATOMIC_RELAXED);
+            while (bits > cur && !__atomic_compare_exchange_n(&colmax[j], &cur, bits, true,
+                                                              __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+            }
+            cur = __atomic_load_n(&colmin[j], __ATOMIC_RELAXED);
+            while (bits < cur && !__atomic_compare_exchange_n(&colmin[j], &cur, bits, true,
+                                                              __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+            }
+        }
+    }
 }
 
 double geometric_factor(double low, double high) {
@@ -489,7 +569,6 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
         if (v == DROP)
             continue;
         const double l = row_l[size_t(i)], u = row_u[size_t(i)];
-        const int64_t b = src.A.ptr[size_t(i)], en = src.A.ptr[size_t(i + 1)];
         if (dupcand[size_t(i)]) {
             const uint64_t h = key_hash[size_t(i)];
             bool merged = false;
@@ -589,37 +668,21 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
     p.row_scale.assign(m.rl.size(), 1);
     if (o.scaling == "combined" && o.scaling_passes > 0)
         geometric_scale(p);
+    // Ruiz passes (src/preprocess.cpp:306-323): the row half and the column
+    // norms in one sweep (ruiz_rows), then the column half (scale_columns)
+    const bool par = m.A.value.size() > 200000 && !g_host_serial;
     for (int pass = 0; pass < o.scaling_passes; pass++) {
-        std::vector<double> row(m.rl.size(), 1), col(m.c.size(), 1);
-        const bool par = m.A.value.size() > 200000 && !g_host_serial;
-#pragma omp parallel for schedule(dynamic, 1024) if (par)
-        for (int64_t ii = 0; ii < int64_t(row.size()); ++ii) {
-            const size_t i = size_t(ii);
-            double norm = 0;
-            for (auto k = m.A.ptr[i]; k < m.A.ptr[i + 1]; ++k)
-                norm = std::max(norm, std::abs(m.A.value[size_t(k)]));
-            row[i] = norm > 0 ? std::clamp(1 / std::sqrt(norm), 1e-3, 1e3) : 1.;
-        }
-        extra_scale(p, row, col);
-        // column maxima: a maximum does not depend on the order it is taken in,
-        // and the bits of non-negative doubles order like their values
-        std::vector<double> norm(col.size());
+        std::vector<uint64_t> colmax(m.c.size(), 0), colmin(m.c.size(), ~uint64_t(0));
+        ruiz_rows(p, par, colmax, colmin);
+        std::vector<double> col(m.c.size());
 #pragma omp parallel for if (par)
-        for (int64_t kk = 0; kk < int64_t(m.A.value.size()); ++kk) {
-            const size_t k = size_t(kk);
-            const double v = std::abs(m.A.value[k]);
-            uint64_t bits, *slot = reinterpret_cast<uint64_t *>(&norm[size_t(m.A.index[k])]);
-            std::memcpy(&bits, &v, 8);
-            uint64_t cur = __atomic_load_n(slot, __ATOMIC_RELAXED);
-            while (bits > cur &&
-                   !__atomic_compare_exchange_n(slot, &cur, bits, true, __ATOMIC_RELAXED,
-                                                __ATOMIC_RELAXED)) {
-            }
+        for (int64_t jj = 0; jj < int64_t(col.size()); ++jj) {
+            const size_t j = size_t(jj);
+            double norm;
+            std::memcpy(&norm, &colmax[j], 8);
+            col[j] = norm > 0 ? std::clamp(1 / std::sqrt(norm), 1e-3, 1e3) : 1.;
         }
-        for (size_t j = 0; j < col.size(); ++j)
-            col[j] = norm[j] > 0 ? std::clamp(1 / std::sqrt(norm[j]), 1e-3, 1e3) : 1.;
-        std::fill(row.begin(), row.end(), 1);
-        extra_scale(p, row, col);
+        scale_columns(p, std::move(col), colmax.data(), colmin.data());
     }
     if (o.scaling == "combined" && o.scaling_passes > 0)
         pock_chambolle_scale(p);

@@ -133,7 +133,22 @@ def infinite_bounds_model():
     return from_rows(9, rows, c=[1, 0.5, -1, 1, 0, -0.5, 1, 1, 0], lb=lb, ub=ub, rl=rl, ru=ru)
 
 
+def subnormal_model():
+    """A column holding the smallest subnormal: its entry would underflow to 0
+    under the column's Ruiz factor, so the column keeps factor 1; and a row
+    whose own factor would zero that entry is left unscaled."""
+    tiny = float(np.nextafter(0.0, 1.0))
+    rows = [[(0, 1e6), (2, 3.0)],
+            [(0, tiny), (1, 1e6)],
+            [(1, 2.0), (2, 5e-3)],
+            [(2, 7.0), (3, tiny * 4)],
+            [(3, 0.5), (0, 2.0)]]
+    return from_rows(4, rows, c=[1, -1, 0.5, 2], lb=[0] * 4, ub=[10] * 4,
+                     rl=[-1, -1, -1, -1, -1], ru=[10, 10, 10, 10, 10])
+
+
 MODELS = {
+    "subnormal": subnormal_model,
     "infinite_bounds": infinite_bounds_model,
     "presolve": presolve_model,
     "presolve_qp": presolve_qp,
