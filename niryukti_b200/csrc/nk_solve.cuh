@@ -22,6 +22,9 @@
 // device evaluation ranks candidates and decides restarts; termination is
 // still certified by the host verifier on the caller's model.
 #pragma once
+#include <exception>
+#include <memory>
+#include <thread>
 
 namespace nk {
 
@@ -766,8 +769,32 @@ inline SolveReport solve(const HostModel &original, const SolveSettings &S) {
     auto start = SteadyClock::now();
     SolveReport R;
     const DriverOptions &o = S.driver;
-    Verifier verifier(original);
-    Prepared prep = prepare(original, S.prepare);
+    // The verifier (its transpose of A) is built on a second host thread while
+    // prepare runs: both only read the caller's model, and prepare's serial
+    // stretches leave host cores free.  The thread follows this thread's
+    // serial-host setting.
+    std::unique_ptr<Verifier> owned_verifier;
+    std::exception_ptr verifier_error;
+    const bool serial = host_serial_enabled();
+    std::thread build_verifier([&] {
+        host_serial(serial);
+        try {
+            owned_verifier = std::make_unique<Verifier>(original);
+        } catch (...) {
+            verifier_error = std::current_exception();
+        }
+    });
+    Prepared prep;
+    try {
+        prep = prepare(original, S.prepare);
+    } catch (...) {
+        build_verifier.join();
+        throw;
+    }
+    build_verifier.join();
+    if (verifier_error)
+        std::rethrow_exception(verifier_error);
+    const Verifier &verifier = *owned_verifier;
     R.preprocess = since(start);
     auto done = [&](int status) {
         R.status = status;

@@ -193,3 +193,26 @@ def test_model_entries_are_checked_like_the_reference():
     m.qval[0] = np.nan
     refused(m, "Invalid quadratic coefficient/index")
     solver.prepare(qp)  # the valid model still passes
+
+
+def test_solve_decided_before_the_device(reference):
+    """nk_solve's host stages (the verifier built beside prepare, the start-point
+    checks of src/solver.cpp:268-287) run without a device: a model infeasible
+    at presolve and one optimal at the start point are decided there, like the
+    reference's solve; any other model then reports the missing device."""
+    from niryukti_b200 import solver
+    from tests.test_host import from_rows
+    infeasible = from_rows(2, [[(0, 2.0)], [(1, 1.0)]], lb=[1, 0], ub=[1, 1], rl=[5, 0],
+                           ru=[6, 1])
+    assert solver.solve(infeasible)["status"] == "INFEASIBLE"
+    assert reference.model(infeasible).solve(method="pdhg")["status"] == "INFEASIBLE"
+    at_start = from_rows(2, [[(0, 1.0), (1, 1.0)]], c=[1, 1], lb=[0, 0], ub=[3, 3],
+                         rl=[-np.inf], ru=[5])
+    r = solver.solve(at_start)
+    want = reference.model(at_start).solve(method="pdhg")
+    assert r["status"] == want["status"] == "OPTIMAL"
+    assert r["iterations"] == 0 and r["objective"] == want["objective"] == 0.0
+    if not engine.cuda_available():
+        with pytest.raises(engine.EngineError) as e:
+            solver.solve(synth.random_lp(m=20, n=40, per_col=2, seed=3))
+        assert e.value.status == "NO_DEVICE"
