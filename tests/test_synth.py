@@ -97,3 +97,31 @@ def test_benchmark_byte_counts():
     primal_q, _ = bench.fused_kernel_bytes(m, n, nnz, diag_q=True)
     assert primal_q == primal + 8 * n
     assert bench.iteration_spmv_bytes(m, n, nnz, s_v=4) == 188_000_004 + 192_000_004
+
+
+def test_reference_arm_json_contract():
+    """`bench.py --impl reference` (CPU: the reference's own CpuBackend) prints
+    one JSON line with the benchmark contract's keys, on the engine arm's
+    metric and workload."""
+    import json
+    import subprocess
+    out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference",
+                          "--scale", "0.01", "--steps", "2", "--warmup", "3", "--no-ref-gpu",
+                          "--ref-trials", "2"], capture_output=True, text=True, timeout=600,
+                         cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+                "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config",
+                "impl", "cpu_baseline", "e2e"):
+        assert key in d, key
+    sys.path.insert(0, str(ROOT))
+    import bench
+    assert d["impl"] == "reference" and d["metric"] == bench.METRIC and d["unit"] == "GB/s"
+    assert d["steps"] == 2 and d["warmup"] == 3 and d["higher_is_better"] is True
+    assert d["config"]["workload"] == "power_law_lp_scaled_0.01" and d["value"] > 0
+    assert set(d["cpu_baseline"]) >= {"value", "unit", "cores", "kind", "sample"}
+    assert d["cpu_baseline"]["value"] == d["value"] == d["e2e"]["value"]
+    assert d["e2e"]["h2d_bytes_per_step"] == d["e2e"]["d2h_bytes_per_step"] == 0
