@@ -16,7 +16,6 @@
 #include <map>
 #include <stdexcept>
 #include <string>
-#include <unordered_map>
 
 namespace nk {
 namespace {
@@ -550,9 +549,15 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
             key_hash[size_t(i)] = row_key_hash(src.A, map, b, en);
         }
     }
-    // first occurrence (prepared row) of each key, by hash; keys are compared in full
-    std::unordered_multimap<uint64_t, size_t> duplicate_rows;
-    duplicate_rows.reserve(size_t(mrows));
+    // first occurrence (prepared row) of each key, by hash; keys are compared in
+    // full.  An open-addressing table (linear probing, at most half full): a
+    // lookup visits every stored row whose hash is equal before it reaches an
+    // empty slot, where a new key goes.
+    size_t slots = 16;
+    while (slots < 2 * size_t(mrows))
+        slots *= 2;
+    std::vector<uint64_t> slot_hash(slots);
+    std::vector<size_t> slot_row(slots, ~size_t(0));
     size_t kept_entries = 0;
     for (int64_t i = 0; i < mrows; i++) {
         const char v = verdict[size_t(i)];
@@ -572,9 +577,11 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
         if (dupcand[size_t(i)]) {
             const uint64_t h = key_hash[size_t(i)];
             bool merged = false;
-            auto range = duplicate_rows.equal_range(h);
-            for (auto it = range.first; it != range.second; ++it) {
-                const size_t r = it->second;
+            size_t slot = size_t(h) & (slots - 1);
+            for (; slot_row[slot] != ~size_t(0); slot = (slot + 1) & (slots - 1)) {
+                if (slot_hash[slot] != h)
+                    continue;
+                const size_t r = slot_row[slot];
                 if (!same_row_key(src.A, map, p.rows[r], i))
                     continue;
                 if (l > m.rl[r]) {
@@ -600,7 +607,8 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
             }
             if (merged)
                 continue;
-            duplicate_rows.emplace(h, p.rows.size());
+            slot_hash[slot] = h;
+            slot_row[slot] = p.rows.size();
         }
         p.rows.push_back(i);
         p.lower_rows.push_back(i);
