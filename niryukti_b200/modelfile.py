@@ -56,8 +56,12 @@ def save(model, path) -> None:
 def load(path) -> synth.Model:
     """Map the model file at `path` and return its model; the arrays are
     read-only views of the mapping and `sense` is -1.0 for a recorded
-    maximisation (else 1.0).  A corrupt, truncated or foreign file
-    raises engine.EngineError (status INVALID) naming the failed check."""
+    maximisation (else 1.0).  The arrays hold the minimisation form, so, as in
+    the reference's Result, solver.solve reports that form's objective;
+    multiply by `sense` for the source objective (serve.result_json does, like
+    the reference's result JSON, src/io.cpp:920).  A corrupt, truncated or
+    foreign file raises engine.EngineError (status INVALID) naming the failed
+    check."""
     path = pathlib.Path(path)
     if path.stat().st_size == 0:
         image = np.zeros(1, dtype=np.uint64)  # let the library report the short file
