@@ -1,6 +1,7 @@
-/* A plain C99 caller of the engine's C ABI, host-only entries (no GPU needed):
+/* A plain C99 caller of the engine's C ABI, runnable with or without a GPU:
  * version check, a model-file round trip, presolve/scaling and the verifier,
- * and the error convention.  Built and run by tests/test_abi.py; it proves that
+ * the batch family's host entries, the solve's missing-device status, and the
+ * error convention.  Built and run by tests/test_abi.py; it proves that
  * include/nk_pdhg.h is valid C and that the library links without C++.
  *
  * The LP: minimise -x0 - x1 subject to x0 + 2 x1 <= 4, 3 x0 + x1 <= 6,
@@ -65,6 +66,29 @@ int main(int argc, char **argv) {
     double accuracy[10];
     if (nk_verify(&view, x, y, 1, accuracy) != NK_OK)
         return fail("nk_verify");
+
+    /* the batch family's host entries: the reference's memory estimate,
+     * 48 B per nonzero + 240 B per row and column, plus two */
+    nk_batch_options batch_options;
+    nk_batch_defaults(&batch_options);
+    double estimate = 0, device_bytes = -1;
+    if (nk_batch_estimate(&view, &estimate) != NK_OK || estimate != 48.0 * 4 + 240.0 * 6)
+        return fail("nk_batch_estimate");
+    nk_batch_item *item = NULL;
+    if (nk_batch_prepare(&view, &batch_options, &item, &device_bytes) != NK_OK || !item ||
+        !(device_bytes > 0))
+        return fail("nk_batch_prepare");
+    nk_batch_item_free(item);
+
+    /* the device-resident solve: OPTIMAL on a GPU, NK_ERR_NO_DEVICE without one */
+    nk_solve_options solve_options;
+    nk_solve_defaults(&solve_options);
+    nk_solve_result result;
+    double sx[2], sy[2];
+    const nk_status solved = nk_solve(&view, &solve_options, &result, sx, sy);
+    if (nk_cuda_available() ? (solved != NK_OK || result.status != NK_SOLVE_OPTIMAL)
+                            : solved != NK_ERR_NO_DEVICE)
+        return fail("nk_solve");
     nk_model_close(file);
 
     if (nk_model_open("/nonexistent/model.nkm", &file, &view, NULL) != NK_ERR_INVALID ||

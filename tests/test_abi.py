@@ -146,7 +146,8 @@ def test_null_pointers_are_argument_errors():
 
 def test_plain_c_caller(tmp_path):
     """include/nk_pdhg.h compiles as strict C99 and a C program linked against
-    the library runs its host-only entries (tests/c/abi_host.c)."""
+    the library runs its host entries and gets the solve's missing-device
+    status (tests/c/abi_host.c)."""
     exe = tmp_path / "abi_host"
     lib_dir = engine.LIB_PATH.parent
     subprocess.check_call(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic",
