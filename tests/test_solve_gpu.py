@@ -199,3 +199,18 @@ def test_sparse_qp_matches_reference(solver, reference):
     assert want["status"] == r["status"] == "OPTIMAL"
     assert r["kkt"] <= TOL
     objective_close(r["objective"], want["objective"])
+
+
+def test_solve_from_model_file(solver, tmp_path):
+    """A model mapped from a model file (read-only views of the mapping, no
+    copy) goes through nk_solve like the in-memory model it was written from."""
+    from niryukti_b200 import modelfile
+    model = synth.random_lp(m=300, n=700, per_col=4, seed=6)
+    modelfile.save(model, tmp_path / "lp.nkm")
+    mapped = modelfile.load(tmp_path / "lp.nkm")
+    assert not mapped.val.flags.writeable  # a view of the mapping
+    a = solver.solve(model, tol=TOL, iteration_limit=200000)
+    b = solver.solve(mapped, tol=TOL, iteration_limit=200000)
+    assert a["status"] == b["status"] == "OPTIMAL", (a["status"], b["status"])
+    assert b["kkt"] <= TOL
+    objective_close(b["objective"], a["objective"])
