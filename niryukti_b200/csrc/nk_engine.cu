@@ -2029,6 +2029,8 @@ nk_status nk_batch_prepare_from(const nk_model *model, const nk_batch_options *o
             throw nk::Error(NK_ERR_INVALID, "null output handle");
         *out = nullptr;
         auto opts = batch_options(o);
+        // requests are prepared concurrently, one per host thread
+        nk::HostSerialScope serial;
         auto host = nk::host_model(model);
         std::vector<double> x, y;
         if (x0)
@@ -2036,7 +2038,6 @@ nk_status nk_batch_prepare_from(const nk_model *model, const nk_batch_options *o
         if (y0)
             y.assign(y0, y0 + host.rl.size());
         auto item = std::make_unique<nk_batch_item>();
-        nk::HostSerialScope serial;
         item->item = nk::batch_prepare(host, opts, x0 ? &x : nullptr, y0 ? &y : nullptr);
         if (device_bytes)
             *device_bytes = item->item->decided ? 0. : double(item->item->bytes);
