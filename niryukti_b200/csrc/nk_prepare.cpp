@@ -252,12 +252,14 @@ void pock_chambolle_scale(Prepared &p) {
 // reference keys a std::map on the same (column, value) vectors; a hash bucket
 // is only a shortlist here, the keys themselves are compared by same_row_key,
 // so equal keys are found alike.
-uint64_t row_key_hash(const Csr &A, const std::vector<int64_t> &map, int64_t b, int64_t en) {
+// `map` null: the identity (no column removed).
+uint64_t row_key_hash(const Csr &A, const int64_t *map, int64_t b, int64_t en) {
     uint64_t h = 1469598103934665603ULL;
     for (auto k = b; k < en; ++k) {
         uint64_t bits;
         std::memcpy(&bits, &A.value[size_t(k)], 8);
-        h = (h ^ uint64_t(map[size_t(A.index[size_t(k)])])) * 1099511628211ULL;
+        const int64_t j = A.index[size_t(k)];
+        h = (h ^ uint64_t(map ? map[j] : j)) * 1099511628211ULL;
         h = (h ^ bits) * 1099511628211ULL;
     }
     return h;
@@ -265,15 +267,17 @@ uint64_t row_key_hash(const Csr &A, const std::vector<int64_t> &map, int64_t b, 
 
 // Equal keys (mapped columns and values, in order) of source rows a and b --
 // the equality the reference's std::map of key vectors applies.
-bool same_row_key(const Csr &A, const std::vector<int64_t> &map, int64_t a, int64_t b) {
+bool same_row_key(const Csr &A, const int64_t *map, int64_t a, int64_t b) {
     const int64_t ba = A.ptr[size_t(a)], ea = A.ptr[size_t(a + 1)];
     const int64_t bb = A.ptr[size_t(b)], eb = A.ptr[size_t(b + 1)];
     if (ea - ba != eb - bb)
         return false;
-    for (int64_t t = 0; t < ea - ba; ++t)
-        if (map[size_t(A.index[size_t(ba + t)])] != map[size_t(A.index[size_t(bb + t)])] ||
+    for (int64_t t = 0; t < ea - ba; ++t) {
+        const int64_t ja = A.index[size_t(ba + t)], jb = A.index[size_t(bb + t)];
+        if ((map ? map[ja] : ja) != (map ? map[jb] : jb) ||
             !(A.value[size_t(ba + t)] == A.value[size_t(bb + t)]))
             return false;
+    }
     return true;
 }
 } // namespace
@@ -468,6 +472,10 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
         }
     const int64_t nk = int64_t(m.c.size());
     m.Q = build_csr(nk, nk, std::move(qe));
+    // No column removed: kept columns are numbered in order, so map[j] == j
+    // and no entry has a fixed-column shift; the loops below skip the map.
+    const bool identity = nk == n;
+    const int64_t *key_map = identity ? nullptr : map.data();
     // Rows in two passes.  The first, row-parallel, does each row's own
     // arithmetic exactly as the reference's loop does (same operations, same
     // order within the row): fixed-column shift, activity bounds, and the
@@ -486,15 +494,18 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
         long double shift = 0, shift_magnitude = 0;
         int64_t count = 0;
         const int64_t b = src.A.ptr[size_t(i)], en = src.A.ptr[size_t(i + 1)];
-        for (auto k = b; k < en; k++) {
-            auto j = src.A.index[size_t(k)];
-            if (map[size_t(j)] < 0) {
-                long double term = (long double)src.A.value[size_t(k)] * p.fixed[size_t(j)];
-                shift += term;
-                shift_magnitude += std::abs(term);
-            } else
-                count++;
-        }
+        if (identity)
+            count = en - b;
+        else
+            for (auto k = b; k < en; k++) {
+                auto j = src.A.index[size_t(k)];
+                if (map[size_t(j)] < 0) {
+                    long double term = (long double)src.A.value[size_t(k)] * p.fixed[size_t(j)];
+                    shift += term;
+                    shift_magnitude += std::abs(term);
+                } else
+                    count++;
+            }
         kept_in_row[size_t(i)] = count;
         double l = src.rl[i] - double(shift), u = src.ru[i] - double(shift);
         row_l[size_t(i)] = l;
@@ -546,7 +557,7 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
         }
         if (o.presolve && count == en - b) {
             dupcand[size_t(i)] = 1;
-            key_hash[size_t(i)] = row_key_hash(src.A, map, b, en);
+            key_hash[size_t(i)] = row_key_hash(src.A, key_map, b, en);
         }
     }
     // first occurrence (prepared row) of each key, by hash; keys are compared in
@@ -582,7 +593,7 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
                 if (slot_hash[slot] != h)
                     continue;
                 const size_t r = slot_row[slot];
-                if (!same_row_key(src.A, map, p.rows[r], i))
+                if (!same_row_key(src.A, key_map, p.rows[r], i))
                     continue;
                 if (l > m.rl[r]) {
                     m.rl[r] = l;
@@ -629,7 +640,8 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
         const int64_t i = p.rows[size_t(r)];
         int64_t last = -1, len = 0;
         for (auto k = src.A.ptr[size_t(i)]; k < src.A.ptr[size_t(i + 1)]; k++) {
-            const int64_t j = map[size_t(src.A.index[size_t(k)])];
+            const int64_t source = src.A.index[size_t(k)];
+            const int64_t j = identity ? source : map[size_t(source)];
             if (j < 0)
                 continue;
             if (j <= last)
@@ -653,7 +665,8 @@ Prepared prepare(const HostModel &src, const PrepareOptions &o) {
             const int64_t i = p.rows[size_t(r)];
             int64_t at = A.ptr[size_t(r)];
             for (auto k = src.A.ptr[size_t(i)]; k < src.A.ptr[size_t(i + 1)]; k++) {
-                const int64_t j = map[size_t(src.A.index[size_t(k)])];
+                const int64_t source = src.A.index[size_t(k)];
+                const int64_t j = identity ? source : map[size_t(source)];
                 if (j >= 0 && src.A.value[size_t(k)] != 0) {
                     A.index[size_t(at)] = j;
                     A.value[size_t(at++)] = src.A.value[size_t(k)];
