@@ -319,6 +319,26 @@ def write_native_json(model, path):
                 % (",".join(map(repr, model.c.tolist())), float(model.offset)))
 
 
+def model_file_timing(model, loads=3):
+    """Writes `model` to a model file in a temporary folder and maps it back
+    (memory map plus the header, size, checksum and CSR checks): seconds of the
+    write and of the best of `loads` loads on a warm page cache."""
+    from niryukti_b200 import modelfile
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "model.nkm")
+        t = time.perf_counter()
+        modelfile.save(model, path)
+        out = {"save_s": time.perf_counter() - t, "file_mb": os.path.getsize(path) / 1e6}
+        best = math.inf
+        for _ in range(loads):
+            t = time.perf_counter()
+            back = modelfile.load(path)
+            best = min(best, time.perf_counter() - t)
+            del back
+        out["load_s"] = best
+    return out
+
+
 def ingest_section(args):
     """Model ingestion of the power-law LP: written to a model file and loaded
     back (memory map plus the header, size, checksum and CSR checks), best of
@@ -327,21 +347,12 @@ def ingest_section(args):
     JSON, and whether it built exactly the arrays the model file holds."""
     from niryukti_b200 import modelfile
     model = build_model(args)
-    out = {"workload": workload_name(args), "m": model.m, "n": model.n, "nnz": model.nnz}
-    with tempfile.TemporaryDirectory() as d:
-        path = os.path.join(d, "model.nkm")
-        t = time.perf_counter()
-        modelfile.save(model, path)
-        out["save_s"] = time.perf_counter() - t
-        out["file_mb"] = os.path.getsize(path) / 1e6
-        loads = []
-        for _ in range(3):
-            t = time.perf_counter()
-            back = modelfile.load(path)
-            loads.append(time.perf_counter() - t)
-            del back
-        out["load_s"] = min(loads)
-        if args.impl == "reference":
+    out = {"workload": workload_name(args), "m": model.m, "n": model.n, "nnz": model.nnz,
+           **model_file_timing(model)}
+    if args.impl == "reference":
+        with tempfile.TemporaryDirectory() as d:
+            path = os.path.join(d, "model.nkm")
+            modelfile.save(model, path)
             from oracle import oracle as orc
             jpath = os.path.join(d, "model.json")
             t = time.perf_counter()
@@ -845,6 +856,13 @@ def engine_arm(args, world, rank, local):
                    "iterations_per_s": c["rate"]}
         except Exception as exc:  # reported, never silently replaced
             cpu = {"error": str(exc)[-500:]}
+    model_file = None
+    if not args.no_ingest:
+        # this host's model-file write and load of the same LP (CPU only)
+        try:
+            model_file = model_file_timing(model)
+        except Exception as exc:  # reported, never raised: the line comes first
+            model_file = {"error": str(exc)[-300:]}
     line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -863,7 +881,7 @@ def engine_arm(args, world, rank, local):
                     "path": "nk_pdhg_reset + nk_pdhg_advance(100) + nk_pdhg_candidates"},
             "gpu_launches": 2 * (args.steps * TRIALS_PER_STEP),
             "clocks": clocks.summary(), "accepted_trials": accepted,
-            "precision_forms": forms}
+            "precision_forms": forms, "model_file": model_file}
     if not args.no_solve:
         line["solve"] = solve_section(args)
     if not args.no_batch:
@@ -924,6 +942,8 @@ def main():
     ap.add_argument("--block-angular", action="store_true",
                     help="print only the block-angular LP iteration-rate section")
     ap.add_argument("--block-angular-blocks", type=int, default=64)
+    ap.add_argument("--no-ingest", action="store_true",
+                    help="skip the model-file write/load timing in the default line")
     ap.add_argument("--ingest", action="store_true",
                     help="time model-file ingestion (and, with --impl reference, the "
                          "reference's JSON reader on the same model); CPU only")
