@@ -37,6 +37,28 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "SpMV HBM GB/s"
 TRIALS_PER_STEP = 100
+# The result line is printed last and kept short: whoever reads the benchmark's
+# output may keep only its tail.  Bulky sections (the batch's per-instance
+# table, the solves, the precision forms) go on earlier lines of their own.
+HEADLINE_MAX_BYTES = 1400
+
+
+def emit(obj) -> None:
+    print(json.dumps(obj), flush=True)
+
+
+def sig(v, digits=4):
+    """v rounded to `digits` significant digits (None, ints and strings pass)."""
+    if not isinstance(v, float) or not math.isfinite(v) or v == 0:
+        return v
+    return round(v, max(0, digits - 1 - int(math.floor(math.log10(abs(v))))))
+
+
+def status_counts(results):
+    out = {}
+    for r in results:
+        out[r] = out.get(r, 0) + 1
+    return out
 
 
 def spmv_bytes(rows, cols, nnz, s_v=8, s_i=4, s_p=4):
@@ -242,15 +264,19 @@ def reference_gpu(args, m, n, nnz):
     try:
         out = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
         if out.returncode != 0:
-            return {"error": out.stderr[-600:]}
+            return {"error": out.stderr[-200:]}
         r = json.loads(out.stdout.strip().splitlines()[-1])
     except Exception as exc:
-        return {"error": str(exc)[-600:]}
+        return {"error": str(exc)[-200:]}
+    return compact_reference_gpu(r, m, n, nnz)
+
+
+def compact_reference_gpu(r, m, n, nnz):
     it_s = r["trials"] / r["seconds"]
-    return {"impl": "reference src/cuda.cu (cuSPARSE), built for sm_100a", "iterations_per_s": it_s,
-            "spmv_GBps": it_s * iteration_spmv_bytes(m, n, nnz) / 1e9,
-            "timing": "wall clock around advance(100) chunks; each ends in the backend's own "
-                      "stream synchronisation", "trials": r["trials"], "seconds": r["seconds"]}
+    return {"impl": "reference src/cuda.cu (cuSPARSE) for sm_100a", "iterations_per_s": sig(it_s),
+            "spmv_GBps": sig(it_s * iteration_spmv_bytes(m, n, nnz) / 1e9),
+            "timing": "wall clock, synchronising advance(100)", "trials": r["trials"],
+            "seconds": sig(r["seconds"])}
 
 
 def reference_arm(args, world, rank):
@@ -286,14 +312,14 @@ def reference_arm(args, world, rank):
                        "nnz": nnz, "trials_per_step": per, "seed": 2},
             "iterations_per_s": rate,
             "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": kind,
-                             "sample": f"{args.steps} steps x {per} PDHG trials of the "
-                                       "power-law LP (adaptive, FP64), CpuBackend::advance"},
+                             "sample": f"{args.steps} steps x {per} adaptive FP64 PDHG trials, "
+                                       "CpuBackend::advance"},
             "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     if not args.no_ref_gpu:
         # beside the CPU arm: the reference's own CUDA build on the same LP, when built
         line["reference_gpu"] = reference_gpu(args, m, n, nnz)
-    print(json.dumps(line))
+    emit(line)
 
 
 # ---------------------------------------------------------------- ingestion
@@ -523,9 +549,12 @@ def batch_section(args):
                       "objective_diff": abs(r["objective"] - results[k]["objective"]) /
                       (1 + abs(r["objective"]))})
     # the sample sits at evenly spaced size quantiles, so its mean time per
-    # instance times the instance count estimates the one-by-one total
+    # instance times the instance count estimates the one-by-one total; its
+    # share of OPTIMAL results estimates how many of them would be certified
     total_nnz = sum(m.nnz for m in models)
     plain_s = sum(p["seconds"] for p in plain) / len(plain) * len(models)
+    plain_opt = sum(p["status"] == "OPTIMAL" for p in plain) / len(plain)
+    n_opt = statuses.get("OPTIMAL", 0)
     out = {"workload": f"uneven_lp_qp_{len(models)}_m500_{args.batch_m_hi}",
            "instances": len(models), "qp": sum(1 for m in models if m.is_qp()),
            "total_nnz": total_nnz, "precision": args.batch_precision, "tol": 1e-6,
@@ -533,12 +562,17 @@ def batch_section(args):
            "iterations": {"min": iters[0], "median": iters[len(iters) // 2], "max": iters[-1]},
            "generate_s": gen_s, "prepare_s_parallel": prep_s, "gpu_phase_s": gpu_s,
            "solves_per_s": len(models) / gpu_s,
+           "optimal_per_s": n_opt / gpu_s,
            "solves_per_s_with_prepare": len(models) / (gpu_s + prep_s),
            "kernel_variants": {"primal": info["primal_variant"], "dual": info["dual_variant"]},
            "check_interval_seconds": phases,
            "plain_fp64_one_by_one": {"sample": plain, "extrapolated_s": plain_s,
-                                     "solves_per_s": len(models) / plain_s},
+                                     "statuses": status_counts(p["status"] for p in plain),
+                                     "solves_per_s": len(models) / plain_s,
+                                     "optimal_per_s": plain_opt * len(models) / plain_s},
            "speedup_vs_plain": plain_s / gpu_s,
+           "speedup_optimal_vs_plain": (n_opt / gpu_s) / (plain_opt * len(models) / plain_s)
+           if plain_opt else None,
            # per instance: m, QP?, status, iterations, reduced-precision iterations,
            # seconds from admission to its result
            "per_instance": [[models[k].m, int(models[k].is_qp()), results[k]["status"][:3],
@@ -851,44 +885,92 @@ def engine_arm(args, world, rank, local):
             c = run_cpu_child(args)
             cpu = {"value": c["rate"] * iteration_spmv_bytes(m, n, nnz) / 1e9, "unit": "GB/s",
                    "cores": c["threads"], "kind": c["kind"],
-                   "sample": f"{c['done']} adaptive FP64 PDHG trials of the same power-law LP in "
-                             f"{c['dt']:.1f} s (CpuBackend::advance, OMP threads {c['threads']})",
+                   "sample": f"{c['done']} adaptive FP64 PDHG trials in {c['dt']:.1f} s "
+                             f"(CpuBackend::advance, {c['threads']} threads)",
                    "iterations_per_s": c["rate"]}
         except Exception as exc:  # reported, never silently replaced
             cpu = {"error": str(exc)[-500:]}
-    model_file = None
-    if not args.no_ingest:
-        # this host's model-file write and load of the same LP (CPU only)
-        try:
-            model_file = model_file_timing(model)
-        except Exception as exc:  # reported, never raised: the line comes first
-            model_file = {"error": str(exc)[-300:]}
+    e2e = {"value": e2e_value, "unit": "GB/s",
+           "h2d_bytes_per_step": 8 * (n + m), "d2h_bytes_per_step": 16 * (n + m)}
     line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32-matrix/f64-iterates",
-            "data": "synthetic (seeded power-law LP, numpy PCG64 seed 2)",
+            "data": "synthetic (seeded power-law LP)",
             "config": {"workload": workload_name(args), "m": m, "n": n, "nnz": nnz,
                        "trials_per_step": TRIALS_PER_STEP, "precision": args.precision,
-                       "adaptive": True, "graphs": True, "parallelism": f"replicas{world}",
-                       "l2": "inputs larger than L2 (about 730 MB per iteration)"},
-            "iterations_per_s": it_s,
-            "whole_iteration_GBps": it_s * (bp + bd) / 1e9,
-            "kernels": kernels, "schedule": sched, "roofline": roofline,
-            "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": "GB/s",
-                    "h2d_bytes_per_step": 8 * (n + m), "d2h_bytes_per_step": 16 * (n + m),
-                    "path": "nk_pdhg_reset + nk_pdhg_advance(100) + nk_pdhg_candidates"},
-            "gpu_launches": 2 * (args.steps * TRIALS_PER_STEP),
-            "clocks": clocks.summary(), "accepted_trials": accepted,
-            "precision_forms": forms, "model_file": model_file}
-    if not args.no_solve:
-        line["solve"] = solve_section(args)
-    if not args.no_batch:
-        line["batch"] = batch_section(args)
-    print(json.dumps(line))
+                       "parallelism": f"replicas{world}", "l2": "inputs > L2"},
+            "iterations_per_s": it_s, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": 2 * (args.steps * TRIALS_PER_STEP), "clocks": clocks.summary()}
+    # the detail first, one section per line; the compact result line last
+    emit({"section": "iteration", "workload": workload_name(args),
+          "iterations_per_s": it_s, "whole_iteration_GBps": it_s * (bp + bd) / 1e9,
+          "kernels": kernels, "schedule": sched, "roofline": roofline, "cpu_baseline": cpu,
+          "e2e": dict(e2e, path="nk_pdhg_reset + nk_pdhg_advance(100) + nk_pdhg_candidates"),
+          "accepted_trials": accepted, "clocks": clocks.summary()})
+    if forms:
+        emit({"section": "precision_forms", **forms})
+    if not args.no_ingest:
+        # this host's model-file write and load of the same LP (CPU only)
+        try:
+            emit({"section": "model_file", **model_file_timing(model)})
+        except Exception as exc:  # reported, never raised: the result line comes last
+            emit({"section": "model_file", "error": str(exc)[-300:]})
+    sections = {}
+    if not args.no_solve and world == 1:
+        sections["solve"] = solve_section(args)
+        emit({"section": "solve", **sections["solve"]})
+    if not args.no_batch and world == 1:
+        sections["batch"] = batch_section(args)
+        emit({"section": "batch", **sections["batch"]})
+    emit(headline(line, sections))
     if dist:
         dist.destroy_process_group()
+
+
+def headline(line, sections):
+    """The result line: the benchmark contract's keys with compact values, plus
+    one-line summaries of the time-to-tolerance solves and of the batch (no
+    arrays; the full sections are printed on the lines before it)."""
+    out = dict(line)
+    for k in ("value", "ms_per_step", "iterations_per_s"):
+        out[k] = sig(out[k], 6)
+    out["roofline"] = {k: sig(v, 5) for k, v in line["roofline"].items()
+                       if k not in ("traffic_source",)}
+    cpu = line.get("cpu_baseline")
+    if cpu and "error" not in cpu:
+        out["cpu_baseline"] = {"value": sig(cpu["value"]), "unit": cpu["unit"],
+                               "cores": cpu["cores"], "kind": cpu["kind"],
+                               "sample": cpu["sample"][:80]}
+    elif cpu:
+        out["cpu_baseline"] = {"error": cpu["error"][-120:]}
+    out["e2e"] = {k: sig(v) for k, v in line["e2e"].items()}
+    ck = line.get("clocks")
+    if ck:
+        out["clocks"] = {"sm_mhz": ck.get("sm_mhz"), "sm_max_mhz": ck.get("sm_max_mhz"),
+                         "reasons": ck.get("reasons")}
+    solve = sections.get("solve")
+    if solve:
+        # per solved LP: status, seconds and KKT reached on the GPU, and the
+        # reference CPU solve's seconds and KKT
+        tt = {}
+        for name, r in solve.items():
+            g = r["gpu"]
+            ref = r.get("reference_cpu") or {}
+            tt[name.split("_m")[0]] = [g["status"][:3], sig(g["seconds"], 3), sig(g["kkt"], 2),
+                                       sig(ref.get("seconds"), 3), sig(ref.get("kkt"), 2)]
+        out["time_to_tol"] = tt
+    b = sections.get("batch")
+    if b:
+        p = b["plain_fp64_one_by_one"]
+        out["batch_summary"] = {
+            "instances": b["instances"], "precision": b["precision"],
+            "statuses": {k[:3]: v for k, v in b["statuses"].items()},
+            "solves_per_s": sig(b["solves_per_s"]), "opt_per_s": sig(b["optimal_per_s"]),
+            "plain_statuses": {k[:3]: v for k, v in p["statuses"].items()},
+            "plain_opt_per_s": sig(p["optimal_per_s"]),
+            "speedup_opt": sig(b["speedup_optimal_vs_plain"], 3)}
+    return out
 
 
 def main():

@@ -337,7 +337,10 @@ nk_status nk_batch_phase_seconds(nk_batch *batch, double seconds[7]);
  * library until the process exits), so n and m are limited to
  * NK_MONITOR_STATIC_MAX entries each; larger inputs fail with NK_ERR_INVALID.
  * The first call on each device looks up that array's device address (and
- * may load the module), so make it before any stream capture.  All calls share
+ * may load the module), so make it before any stream capture.  The address is
+ * kept for the life of the process: after cudaDeviceReset (or any other
+ * teardown of the device's primary context) the array may move, and calls
+ * made after such a reset are not supported.  All calls share
  * the array: the counter is cleared on `stream` before every launch, and calls
  * whose kernels can overlap on the GPU (different streams, or different host
  * threads) race and must be serialised by the caller. */

@@ -1475,8 +1475,8 @@ nk_status nk_pdhg_monitor(nk_pdhg *h, double *out) {
 // ---- KKT proxy on fixed library scratch (see nk_monitor_static in nk_pdhg.h).
 // Callers that may not allocate device memory get the monitor kernel launched
 // on this array instead of engine buffers: bytes [0, 256) hold the kernel's
-// arrival counter, the rest five partial sums per block, one block per
-// kThreads entries of the longer vector.
+// arrival counter, the rest five partial sums per block (room for one block
+// per kThreads entries of NK_MONITOR_STATIC_MAX; a launch uses at most 1184).
 namespace {
 constexpr int64_t kStaticMonitorBlocks = NK_MONITOR_STATIC_MAX / nk::kThreads;
 constexpr size_t kStaticMonitorBytes = 256 + size_t(kStaticMonitorBlocks) * 5 * sizeof(double);
@@ -1526,7 +1526,9 @@ nk_status nk_monitor_static(int64_t n, int64_t m, const double *x, const double 
             nk::cuda_check(cudaMemsetAsync(result, 0, sizeof(double), s), "result");
             return;
         }
-        const int blocks = int((top + nk::kThreads - 1) / nk::kThreads);
+        // the grid of nk_pdhg_monitor (the kernel is grid-stride): at most
+        // 1184 blocks, whose partials the last block adds serially
+        const int blocks = nk::grid_for(top);
         // a call that ended early must not leave a stale count behind
         nk::cuda_check(cudaMemsetAsync(arrive, 0, sizeof(unsigned), s), "clear counter");
         nk::monitor_kernel<<<blocks, nk::kThreads, 0, s>>>(n, m, x, y, ax, aty, qx, c, q, lb, ub,

@@ -268,3 +268,42 @@ def test_oracle_propagation_known_answers(oracle):
     m = _one_row([1, -1], [0, -np.inf], [5, np.inf], 0, 2)
     ok, lb, ub = oracle.propagate_bounds(m, [0, 0], m.lb, m.ub)
     assert ok and lb.tolist() == [0.0, -2.0] and ub.tolist() == [5.0, 5.0]
+
+
+def test_monitor_formula_known_answer():
+    """The host restatement of the reference's GPU KKT proxy
+    (src/cuda.cu:387-446) on the sparse QP of tests/test_research.cpp:118-125
+    at x = (1, 1), y = 0.5, worked by hand: A x = 2 against rl = ru = 3 gives a
+    row violation 1/4; g = c + Q x + A^T y = (-0.5, -1.5) gives dual residuals
+    0.5/6 and 1.5/6 (cscale = 1 + 5); complementarity 0.5*3 + 1.5*3 + 0.5*(3-2)
+    = 6.5 over 1 + |c.x + x'Qx/2| = 1 + |-9 + 3| = 7."""
+    from oracle.monitor import cscale_of, monitor, monitor_point
+    m = sparse_qp_model()
+    x, y = np.array([1.0, 1.0]), np.array([0.5])
+    assert cscale_of(m.c) == 6.0
+    assert monitor_point(m, x, y) == pytest.approx(6.5 / 7, rel=1e-15)
+    # at the optimum (1, 2) with y = 0 every term vanishes
+    assert monitor_point(m, np.array([1.0, 2.0]), np.zeros(1)) == 0.0
+    assert monitor(m, x, y, np.array([1.0, 2.0]), np.zeros(1)) == 0.0
+    # a bound violation relative to 1 + |x|, and a non-finite point
+    assert monitor_point(m, np.array([5.0, -2.0]), np.zeros(1)) >= 1.0 / 6
+    assert monitor_point(m, np.array([np.nan, 1.0]), np.zeros(1)) == np.inf
+
+
+def test_monitor_formula_infinite_endpoints():
+    """Rows with an infinite endpoint: a dual sign that selects it counts |y_i|
+    as a dual residual (src/cuda.cu:414-420); a finite one counts
+    complementarity.  One free column at x = 2, c = 0, rows x >= 1 and x <= 4."""
+    from oracle.monitor import monitor_point
+    m = tiny(1, 2, [(0, 0, 1.0), (1, 0, 1.0)])
+    m.lb[:], m.ub[:] = -math.inf, math.inf
+    m.rl = np.array([1.0, -math.inf])
+    m.ru = np.array([math.inf, 4.0])
+    x = np.array([2.0])
+    # g = A^T y = 0.25 is the column's dual residual; y_0 < 0 selects rl = 1:
+    # 0.25 * |1 - 2|; y_1 > 0 selects ru = 4: 0.5 * |4 - 2|; over 1 + |0|
+    assert monitor_point(m, x, np.array([-0.25, 0.5])) == 1.25
+    # y_0 > 0 selects ru = +inf: |y_0| = 3 is a dual residual (and so is g = 3)
+    assert monitor_point(m, x, np.array([3.0, 0.0])) == 3.0
+    # a row violation relative to 1 + |rl|: x = 0.5 against rl = 1
+    assert monitor_point(m, np.array([0.5]), np.zeros(2)) == 0.25

@@ -112,6 +112,9 @@ def test_reference_arm_json_contract():
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1
+    sys.path.insert(0, str(ROOT))
+    import bench
+    assert len(lines[0]) <= bench.HEADLINE_MAX_BYTES
     d = json.loads(lines[0])
     for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
                 "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config",
@@ -125,3 +128,80 @@ def test_reference_arm_json_contract():
     assert set(d["cpu_baseline"]) >= {"value", "unit", "cores", "kind", "sample"}
     assert d["cpu_baseline"]["value"] == d["value"] == d["e2e"]["value"]
     assert d["e2e"]["h2d_bytes_per_step"] == d["e2e"]["d2h_bytes_per_step"] == 0
+
+
+def _fake_engine_line():
+    """An engine-arm result with every key at its widest realistic value."""
+    sample = [{"instance": k, "m": 50000, "nnz": 600000, "seconds": 12.345678, "status": s,
+               "iterations": 100062, "objective_diff": 1.234e-9}
+              for k, s in enumerate(["OPTIMAL", "ITERATION_LIMIT"] * 8)]
+    line = {"metric": "SpMV HBM GB/s", "value": 2868.123456789, "unit": "GB/s", "n_gpus": 1,
+            "steps": 20, "warmup": 5, "ms_per_step": 18.83123456789, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded power-law LP)",
+            "config": {"workload": "power_law_lp_m1e6_n2e6_nnz2e7", "m": 1000000,
+                       "n": 2000000, "nnz": 20000000, "trials_per_step": 100,
+                       "precision": "fp64", "parallelism": "replicas1",
+                       "l2": "inputs > L2"},
+            "iterations_per_s": 5310.123456789,
+            "roofline": {"bound": "hbm", "kernel": "dual_kernel", "achieved": 2830.123456789,
+                         "peak": 6468.6, "unit": "GB/s", "frac": 0.4375123456789,
+                         "traffic": 332480000.0, "traffic_source": "x" * 80,
+                         "peak_source": "measured"},
+            "cpu_baseline": {"value": 43.933106912192, "unit": "GB/s", "cores": 16,
+                             "kind": "reference", "sample": "y" * 200,
+                             "iterations_per_s": 81.357},
+            "e2e": {"value": 2624.123456789, "unit": "GB/s", "h2d_bytes_per_step": 24000000,
+                    "d2h_bytes_per_step": 48000000},
+            "gpu_launches": 4000,
+            "clocks": {"sm_mhz": 1927.0, "sm_max_mhz": 1965.0,
+                       "reasons": ["sw_power_cap"], "samples": 1879}}
+    solve = {name: {"gpu": {"status": "ITERATION_LIMIT", "seconds": 60.123456, "kkt": 2.0123e-2},
+                    "reference_cpu": {"status": "TIME_LIMIT", "seconds": 32.3456, "kkt": 5.123}}
+             for name in ("random_lp_m2000_n5000", "power_law_lp_m1e6_n2e6_nnz2e7")}
+    batch = {"instances": 512, "precision": "mixed", "gpu_phase_s": 110.123456,
+             "statuses": {"OPTIMAL": 312, "ITERATION_LIMIT": 199, "PRIMAL_INFEASIBLE": 1},
+             "solves_per_s": 4.6543210, "optimal_per_s": 2.8345678,
+             "speedup_optimal_vs_plain": 5.123456,
+             "plain_fp64_one_by_one": {"sample": sample, "optimal_per_s": 0.4123456,
+                                       "statuses": {"OPTIMAL": 10, "ITERATION_LIMIT": 6}},
+             "per_instance": [[50000, 1, "OPT", 100062, 9999, 101.98]] * 512}
+    return line, {"solve": solve, "batch": batch}
+
+
+def test_headline_line_is_compact_and_complete():
+    """The engine arm's last line stays short enough for a reader that keeps only
+    the tail of the output, and still carries the contract's keys and the
+    solve/batch summaries (the bulky sections go on earlier lines)."""
+    import json
+    sys.path.insert(0, str(ROOT))
+    import bench
+    line, sections = _fake_engine_line()
+    h = bench.headline(line, sections)
+    text = json.dumps(h)
+    assert len(text) <= bench.HEADLINE_MAX_BYTES, len(text)
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+                "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config",
+                "roofline", "cpu_baseline", "e2e", "gpu_launches", "clocks"):
+        assert key in h, key
+    assert set(h["roofline"]) >= {"bound", "achieved", "peak", "unit", "frac", "traffic"}
+    assert set(h["cpu_baseline"]) >= {"value", "unit", "cores", "kind", "sample"}
+    assert set(h["e2e"]) == {"value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step"}
+    assert h["value"] == pytest.approx(line["value"], rel=1e-5)
+    assert h["batch_summary"]["statuses"]["OPT"] == 312
+    assert "per_instance" not in text and "sample\": [" not in text
+    assert json.loads(text) == h
+
+
+def test_reference_arm_line_is_compact():
+    sys.path.insert(0, str(ROOT))
+    import bench
+    line, _ = _fake_engine_line()
+    ref = {k: line[k] for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup",
+                                "ms_per_step", "higher_is_better", "scaling", "vs_baseline",
+                                "dtype", "data", "config", "cpu_baseline", "e2e")}
+    ref["reference_gpu"] = bench.compact_reference_gpu(
+        {"trials": 2000, "seconds": 0.6865915209999969}, 1000000, 2000000, 20000000)
+    ref["cpu_baseline"]["sample"] = ref["cpu_baseline"]["sample"][:110]
+    import json
+    assert len(json.dumps(ref)) <= bench.HEADLINE_MAX_BYTES
