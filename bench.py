@@ -129,6 +129,8 @@ class Clocks:
                 self.proc.kill()
 
     def summary(self):
+        if getattr(self, "_summary", None) is not None:
+            return self._summary
         if not self.file:
             return None
         self.file.flush()
@@ -145,9 +147,10 @@ class Clocks:
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(rows)}
+        self._summary = {"sm_mhz": statistics.median(sm) if sm else None,
+                         "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                         "samples": len(rows)}
+        return self._summary
 
 
 def max_over_ranks(value: float, dist=None, device: str = "cuda") -> float:
@@ -492,6 +495,59 @@ def solve_section(args):
     return res
 
 
+# ---------------------------------------------------------------- KKT at equal iterations
+CURVE_KEYS = ("status", "iterations", "kkt", "primal", "dual", "gap", "objective", "seconds",
+              "preprocess_seconds")
+
+
+def kkt_curve_child(args):
+    """(child process) The reference's own solve of the power-law LP (vantage::solve,
+    method pdhg, default options) capped at each of --curve-iters iterations:
+    --curve-device cpu runs its CPU backend on --cpu-threads threads, cuda its
+    CUDA build (src/cuda.cu for sm_100a, CUDA graphs on)."""
+    from oracle import oracle as orc
+    model = build_model(args)
+    path = orc.REF_CUDA_SO if args.curve_device == "cuda" else orc.REF_SO
+    ref = orc.Reference(path).model(model)
+    out = []
+    for cap in args.curve_iters:
+        r = ref.solve(method="pdhg", device=args.curve_device, threads=args.cpu_threads,
+                      iteration_limit=cap, time_limit=1e6,
+                      cuda_graphs=args.curve_device == "cuda")
+        out.append({"cap": cap, **{k: r[k] for k in CURVE_KEYS}})
+    print(json.dumps(out))
+
+
+def kkt_curve_section(args):
+    """KKT reached at equal iteration counts on the power-law LP: the engine's
+    device-resident solve (FP64), the reference's CPU solve and the reference's
+    CUDA build, each stopped by the same iteration limit (the reference's
+    default options otherwise: adaptive steps, restarts, checks every 100)."""
+    from niryukti_b200 import solver
+    model = build_model(args)
+    out = {"workload": workload_name(args), "engine": []}
+    for cap in args.curve_iters:
+        r = solver.solve(model, tol=1e-6, time_limit=1e6, iteration_limit=cap,
+                         matrix_precision="fp64")
+        out["engine"].append({"cap": cap, **{k: r[k] for k in CURVE_KEYS}})
+    from oracle import oracle as orc
+    for dev, so in (("cuda", orc.REF_CUDA_SO), ("cpu", orc.REF_SO)):
+        if args.no_cpu and dev == "cpu" or not so.exists():
+            continue
+        cmd = [sys.executable, str(pathlib.Path(__file__).resolve()), "--kkt-curve-child",
+               "--curve-device", dev, "--cpu-threads", str(args.cpu_threads), "--scale",
+               str(args.scale), "--curve-iters", *map(str, args.curve_iters)]
+        env = dict(os.environ, OMP_NUM_THREADS=str(args.cpu_threads))
+        try:
+            res = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=3600)
+            out[f"reference_{dev}"] = json.loads(res.stdout.strip().splitlines()[-1]) \
+                if res.returncode == 0 else {"error": res.stderr[-500:]}
+        except Exception as exc:
+            out[f"reference_{dev}"] = {"error": str(exc)[-300:]}
+    out["reference_cpu_threads"] = args.cpu_threads
+    return out
+
+
 # ---------------------------------------------------------------- batch (512 uneven LP/QP instances)
 def batch_models(args):
     from niryukti_b200 import synth
@@ -711,6 +767,22 @@ def synth_pool(args):
 
 # ---------------------------------------------------------------- engine arm
 S_V = {"fp64": 8, "mixed": 4, "fp32": 4}
+# DRAM bytes (read + write) per launch of each step of the power-law LP at
+# scale 0.5 from one ncu capture of the current kernels (the capture is named in
+# profiles/); the dual step is the panel kernel plus the dual kernel
+HALF_SCALE_TRAFFIC = {}
+
+
+def step_kernels(g, model, s_v, trials, tau, sigma):
+    """CUDA-event durations of a trial's steps over `trials` single trials: the
+    primal kernel, and the dual step (the panel kernel, when A's long rows are
+    stored by column panel, plus the dual kernel), each with the algorithmic
+    bytes of fused_kernel_bytes."""
+    bp, bd = fused_kernel_bytes(model.m, model.n, model.nnz, s_v, diag_q=bool(np.any(model.q)))
+    ms_p, ms_k, ms_d = g.profile_kernels(trials, tau, sigma)
+    return {"primal_kernel": {"ms": ms_p, "bytes": bp, "GBps": bp / ms_p / 1e6},
+            "dual_step": {"ms": ms_k + ms_d, "bytes": bd, "GBps": bd / (ms_k + ms_d) / 1e6,
+                          "panel_kernel_ms": ms_k, "dual_kernel_ms": ms_d}}
 
 
 def time_form(model, precision, steps, warmup, profile_trials):
@@ -737,15 +809,13 @@ def time_form(model, precision, steps, warmup, profile_trials):
         ms = e0.elapsed_time(e1)
         it_s = steps * TRIALS_PER_STEP / (ms / 1e3)
         s_v = S_V[precision]
-        ms_p, ms_d = g.profile(profile_trials, tau, sigma)
-        bp, bd = fused_kernel_bytes(m, n, nnz, s_v, diag_q=bool(np.any(model.q)))
+        kernels = step_kernels(g, model, s_v, profile_trials, tau, sigma)
+        bp, bd = kernels["primal_kernel"]["bytes"], kernels["dual_step"]["bytes"]
         return {"matrix_precision": precision, "iterations_per_s": it_s,
                 "ms_per_iteration": 1e3 / it_s,
                 "spmv_GBps": it_s * iteration_spmv_bytes(m, n, nnz, s_v) / 1e9,
                 "whole_iteration_GBps": it_s * (bp + bd) / 1e9,
-                "kernels": {"primal_kernel": {"ms": ms_p, "bytes": bp, "GBps": bp / ms_p / 1e6},
-                            "dual_kernel": {"ms": ms_d, "bytes": bd, "GBps": bd / ms_d / 1e6}},
-                "schedule": g.schedule_info()}
+                "kernels": kernels, "layout": g.layout_info()}
     finally:
         del g
         torch.cuda.synchronize()
@@ -819,10 +889,9 @@ def engine_arm(args, world, rank, local):
     value = replica_rate(world, trials, ms) * iteration_spmv_bytes(m, n, nnz, s_v) / 1e9
 
     # per-kernel durations (CUDA events around each kernel, same stream)
-    ms_p, ms_d = g.profile(args.profile_trials, tau, sigma)
-    bp, bd = fused_kernel_bytes(m, n, nnz, s_v, diag_q=bool(np.any(model.q)))
-    kernels = {"primal_kernel": {"ms": ms_p, "bytes": bp, "GBps": bp / ms_p / 1e6},
-               "dual_kernel": {"ms": ms_d, "bytes": bd, "GBps": bd / ms_d / 1e6}}
+    layout = g.layout_info()
+    kernels = step_kernels(g, model, s_v, args.profile_trials, tau, sigma)
+    bp, bd = kernels["primal_kernel"]["bytes"], kernels["dual_step"]["bytes"]
     top = max(kernels, key=lambda k: kernels[k]["ms"])
     peaks = {}
     pk = ROOT / "MEASURED_PEAKS.json"
@@ -830,11 +899,12 @@ def engine_arm(args, world, rank, local):
         peaks = json.loads(pk.read_text())
     peak = float(peaks.get("hbm_gbs", 6650.0))
     traffic, traffic_source = args.traffic, "--traffic" if args.traffic else None
-    if traffic is None and args.precision == "fp64" and not args.small and args.scale == 1.0:
+    if traffic is None and args.precision == "fp64" and not args.small and args.scale == 1.0 \
+            and top in HALF_SCALE_TRAFFIC:
         # DRAM bytes per launch from the ncu capture of the power-law LP at half
-        # size (profiles/fused_pdhg_kernels_power_law_lp_half_scale.md: read + write),
-        # scaled by 2: every unit (nonzeros, rows, columns) doubles
-        traffic = {"primal_kernel": 2 * 181.32e6, "dual_kernel": 2 * 166.24e6}[top]
+        # size (read + write, summed over the step's kernels), scaled by 2: every
+        # unit (nonzeros, rows, columns) doubles
+        traffic = 2 * HALF_SCALE_TRAFFIC[top]
         traffic_source = "ncu dram__bytes_read.sum + dram__bytes_write.sum at scale 0.5, x2"
     roofline = {"bound": "hbm", "kernel": top, "achieved": kernels[top]["GBps"], "peak": peak,
                 "unit": "GB/s", "frac": kernels[top]["GBps"] / peak, "traffic": traffic,
@@ -890,6 +960,7 @@ def engine_arm(args, world, rank, local):
                    "iterations_per_s": c["rate"]}
         except Exception as exc:  # reported, never silently replaced
             cpu = {"error": str(exc)[-500:]}
+    clock_summary = clocks.summary()
     e2e = {"value": e2e_value, "unit": "GB/s",
            "h2d_bytes_per_step": 8 * (n + m), "d2h_bytes_per_step": 16 * (n + m)}
     line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
@@ -901,13 +972,15 @@ def engine_arm(args, world, rank, local):
                        "trials_per_step": TRIALS_PER_STEP, "precision": args.precision,
                        "parallelism": f"replicas{world}", "l2": "inputs > L2"},
             "iterations_per_s": it_s, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": 2 * (args.steps * TRIALS_PER_STEP), "clocks": clocks.summary()}
+            "gpu_launches": layout["kernels_per_trial"] * (args.steps * TRIALS_PER_STEP),
+            "clocks": clock_summary}
     # the detail first, one section per line; the compact result line last
     emit({"section": "iteration", "workload": workload_name(args),
           "iterations_per_s": it_s, "whole_iteration_GBps": it_s * (bp + bd) / 1e9,
-          "kernels": kernels, "schedule": sched, "roofline": roofline, "cpu_baseline": cpu,
+          "kernels": kernels, "schedule": sched, "layout": layout, "roofline": roofline,
+          "cpu_baseline": cpu,
           "e2e": dict(e2e, path="nk_pdhg_reset + nk_pdhg_advance(100) + nk_pdhg_candidates"),
-          "accepted_trials": accepted, "clocks": clocks.summary()})
+          "accepted_trials": accepted, "clocks": clock_summary})
     if forms:
         emit({"section": "precision_forms", **forms})
     if not args.no_ingest:
@@ -917,12 +990,14 @@ def engine_arm(args, world, rank, local):
         except Exception as exc:  # reported, never raised: the result line comes last
             emit({"section": "model_file", "error": str(exc)[-300:]})
     sections = {}
-    if not args.no_solve and world == 1:
-        sections["solve"] = solve_section(args)
-        emit({"section": "solve", **sections["solve"]})
-    if not args.no_batch and world == 1:
-        sections["batch"] = batch_section(args)
-        emit({"section": "batch", **sections["batch"]})
+    for name, run in (("solve", solve_section), ("batch", batch_section)):
+        if getattr(args, f"no_{name}") or world != 1:
+            continue
+        try:
+            sections[name] = run(args)
+            emit({"section": name, **sections[name]})
+        except Exception as exc:  # reported; the result line still comes last
+            emit({"section": name, "error": repr(exc)[-500:]})
     emit(headline(line, sections))
     if dist:
         dist.destroy_process_group()
@@ -1029,10 +1104,17 @@ def main():
     ap.add_argument("--ingest", action="store_true",
                     help="time model-file ingestion (and, with --impl reference, the "
                          "reference's JSON reader on the same model); CPU only")
+    ap.add_argument("--kkt-curve", action="store_true",
+                    help="print only the KKT reached at equal iteration counts (engine, "
+                         "reference CPU, reference CUDA build) on the power-law LP")
+    ap.add_argument("--kkt-curve-child", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--curve-device", default="cpu", choices=["cpu", "cuda"],
+                    help=argparse.SUPPRESS)
+    ap.add_argument("--curve-iters", type=int, nargs="+", default=[2000, 10000])
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per launch of the top kernel from an ncu capture")
     args = ap.parse_args()
-    if args.warmup < 3 and not (args.cpu_child or args.solve_child):
+    if args.warmup < 3 and not (args.cpu_child or args.solve_child or args.kkt_curve_child):
         ap.error("--warmup must be at least 3")
     if args.cpu_child:
         return cpu_child(args)
@@ -1040,6 +1122,11 @@ def main():
         return ref_gpu_child(args)
     if args.solve_child:
         return solve_child(args)
+    if args.kkt_curve_child:
+        return kkt_curve_child(args)
+    if args.kkt_curve:
+        print(json.dumps({"kkt_curve": kkt_curve_section(args)}))
+        return
     if args.batch_only:
         print(json.dumps({"batch": batch_throughput(args) if args.batch_trials
                           else batch_section(args)}))

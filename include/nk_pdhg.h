@@ -121,9 +121,21 @@ nk_status nk_pdhg_stats(nk_pdhg *h, int64_t *trials, int64_t *device_bytes);
 /* Profiling (no reference counterpart): runs `count` trials one at a time with
  * CUDA events around each kernel on the engine's stream and returns the mean
  * duration of the fused primal (A^T y + primal step) and dual (A dx + dual step
- * + decision) kernels in milliseconds.  The trials advance the iterate. */
+ * + decision) steps in milliseconds; the dual step includes the panel kernel
+ * when A's long rows are stored by column panel.  The trials advance the
+ * iterate. */
 nk_status nk_pdhg_profile(nk_pdhg *h, int count, double tau, double sigma, double *ms_primal,
                           double *ms_dual);
+/* The same, kernel by kernel: ms[0] the primal kernel, ms[1] the panel kernel
+ * (0 when A has no panels), ms[2] the dual kernel. */
+nk_status nk_pdhg_profile_kernels(nk_pdhg *h, int count, double tau, double sigma,
+                                  double ms[3]);
+/* Layout of the dual SpMV (no reference counterpart): how many of A's rows
+ * (its longest, past the SELL split length) are stored by column panel, the
+ * panel width in columns, the number of panels (all 0 without panels), and
+ * the kernel launches per trial.  Null outputs are skipped. */
+nk_status nk_pdhg_layout_info(nk_pdhg *h, int64_t *long_rows, int64_t *panel_width,
+                              int *panels, int *kernels_per_trial);
 /* Profiling (no reference counterpart): mean duration in milliseconds of `reps`
  * plain SpMVs (no fused epilogue) with A (which = 0, input x) or A^T (which = 1,
  * input y) on the resident iterate; results go to scratch, iterates unchanged. */

@@ -869,7 +869,7 @@ class Batch {
     // kernel variant v (autotuned): run length {1, 4, 16}[v / 9], unroll
     // {2, 4, 8}[v / 3 % 3], CTA size {128, 256, 512}[v % 3]
     static constexpr int kVariants = 27;
-    void launch_half(int v, bool primal) {
+    void launch_half(int v, bool primal, bool probe = false) {
         static const int threads_of[3] = {128, 256, 512};
         const int threads = threads_of[v % 3], u = v / 3 % 3, r = v / 9;
         const int items = primal ? nwc_[r] : nwr_[r];
@@ -880,10 +880,12 @@ class Batch {
                                               sms_ * (2048 / threads)));
         if (primal) {
             auto *k = u == 0 ? batch_primal<2> : u == 1 ? batch_primal<4> : batch_primal<8>;
-            k<<<grid, threads, 0, stream_>>>(d_ins_.p, d_ctl_.p, d_wcols_[r].p, items, d_pp_.p);
+            k<<<grid, threads, 0, stream_>>>(d_ins_.p, d_ctl_.p, d_wcols_[r].p, items, d_pp_.p,
+                                             int(probe));
         } else {
             auto *k = u == 0 ? batch_dual<2> : u == 1 ? batch_dual<4> : batch_dual<8>;
-            k<<<grid, threads, 0, stream_>>>(d_ins_.p, d_ctl_.p, d_wrows_[r].p, items, d_pd_.p);
+            k<<<grid, threads, 0, stream_>>>(d_ins_.p, d_ctl_.p, d_wrows_[r].p, items, d_pd_.p,
+                                             int(probe));
         }
     }
     void launch_decide() {
@@ -900,26 +902,27 @@ class Batch {
         cuda_check(cudaGetLastError(), "batch trial");
     }
 
-    // Autotuner: times every kernel variant on the batch as it stands (the
-    // trials are real PDHG trials; every variant computes the same sums in the
-    // same order) and keeps the fastest primal and dual variants.
+    // Autotuner: times every kernel variant on the batch as it stands and
+    // keeps the fastest primal and dual variants (every variant computes the
+    // same sums in the same order).  The timed launches are probe trials: they
+    // do a trial's work on the current iterates but apply no pending average
+    // and make no decision, so the instances' iterates, averages and step
+    // state come out of tuning untouched and every trajectory is the one it
+    // would have been without it.
     void autotune() {
         push_steps();
         cudaEvent_t e0, e1;
         cuda_check(cudaEventCreate(&e0), "event");
         cuda_check(cudaEventCreate(&e1), "event");
-        // every timed launch is part of a complete trial (primal, dual, decide)
+        // a timed dual launch follows a probe primal launch (it reads that dx)
         auto time_half = [&](int v, bool primal) {
             float best = 1e30f;
             for (int rep = 0; rep < 3; ++rep) {
                 if (!primal)
-                    launch_half(vp_, true);
+                    launch_half(vp_, true, true);
                 cuda_check(cudaEventRecord(e0, stream_), "event");
-                launch_half(v, primal);
+                launch_half(v, primal, true);
                 cuda_check(cudaEventRecord(e1, stream_), "event");
-                if (primal)
-                    launch_half(vd_, false);
-                launch_decide();
                 cuda_check(cudaEventSynchronize(e1), "event");
                 float ms = 0;
                 cudaEventElapsedTime(&ms, e0, e1);

@@ -130,10 +130,14 @@ __device__ __forceinline__ double chunk_q(const BInst &I, bool f64, int j, bool 
     return qa;
 }
 
-// part[w.part + k] = sum dx^2 of chunk k of the run.
+// part[w.part + k] = sum dx^2 of chunk k of the run.  With `probe` (the
+// autotuner's timed trials) a pending average is left pending: the launch then
+// writes only the trial buffers, dx and the partials, which the next trial
+// overwrites, so it leaves no trace in any instance's trajectory.
 template <int U>
 __global__ void batch_primal(const BInst *__restrict__ ins, const BCtl *__restrict__ ctl,
-                             const BWork *__restrict__ work, int nwork, double *part) {
+                             const BWork *__restrict__ work, int nwork, double *part,
+                             int probe) {
     const int lane = threadIdx.x & 31;
     const int warps = int((int64_t(gridDim.x) * blockDim.x) >> 5);
     for (int w = int((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5); w < nwork; w += warps) {
@@ -148,7 +152,7 @@ __global__ void batch_primal(const BInst *__restrict__ ins, const BCtl *__restri
         const bool f64 = s.fp64 != 0;
         const int cur = s.cur, n = I.n;
         const double tau = s.tau * s.factor, pw = s.pending_w;
-        const bool pending = s.pending != 0, sq = I.q_ptr != nullptr;
+        const bool pending = s.pending != 0 && !probe, sq = I.q_ptr != nullptr;
         const double *x = I.x[cur], *y = I.y[cur];
         double *xt = I.x[cur ^ 1];
         for (int k = 0; k < it.count; ++k) {
@@ -182,9 +186,10 @@ __global__ void batch_primal(const BInst *__restrict__ ins, const BCtl *__restri
 }
 
 // part[2 (w.part + k)] = sum dy^2, part[2 (w.part + k) + 1] = sum dy * delta.
+// `probe` as for batch_primal.
 template <int U>
 __global__ void batch_dual(const BInst *__restrict__ ins, const BCtl *__restrict__ ctl,
-                           const BWork *__restrict__ work, int nwork, double *part) {
+                           const BWork *__restrict__ work, int nwork, double *part, int probe) {
     const int lane = threadIdx.x & 31;
     const int warps = int((int64_t(gridDim.x) * blockDim.x) >> 5);
     for (int w = int((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5); w < nwork; w += warps) {
@@ -201,7 +206,7 @@ __global__ void batch_dual(const BInst *__restrict__ ins, const BCtl *__restrict
         const bool f64 = s.fp64 != 0;
         const int cur = s.cur, m = I.m;
         const double sigma = s.sigma * s.factor, pw = s.pending_w;
-        const bool pending = s.pending != 0;
+        const bool pending = s.pending != 0 && !probe;
         const double *y = I.y[cur], *ax = I.ax[cur];
         double *yt = I.y[cur ^ 1], *axt = I.ax[cur ^ 1];
         for (int k = 0; k < it.count; ++k) {

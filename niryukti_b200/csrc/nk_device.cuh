@@ -20,9 +20,13 @@
 #include "nk_sell.cuh"
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <type_traits>
 
-#ifndef NK_MIN_BLOCKS
-#define NK_MIN_BLOCKS 4 // CTAs per SM the fused kernels are register-bounded for
+#ifndef NK_FUSED_THREADS
+#define NK_FUSED_THREADS 1024 // threads per CTA of the fused trial kernels
+#endif
+#ifndef NK_HOT
+#define NK_HOT 0 // 1: the primal kernel gathers y's leading entries from shared memory
 #endif
 #ifndef NK_SPLIT_PIPE
 #define NK_SPLIT_PIPE 0 // 1: software-pipelined dot for split-row segments
@@ -37,6 +41,12 @@
 namespace nk {
 
 constexpr int kDualGather = NK_DUAL_GATHER;
+// The fused kernels run 1024 threads per SM (64 registers each) in CTAs of
+// kFusedThreads; larger CTAs give each CTA a larger slice of shared memory.
+constexpr int kFusedThreads = NK_FUSED_THREADS;
+constexpr int kFusedWarps = kFusedThreads / 32;
+constexpr int kFusedMinBlocks = 1024 / kFusedThreads;
+static_assert(kFusedThreads % 32 == 0 && 1024 % kFusedThreads == 0, "fused CTA size");
 
 // Device-resident control state.  The first eleven fields keep the meaning of
 // the reference's `state` vector (src/cuda.cu:224-225,601).
@@ -72,6 +82,11 @@ struct Vecs {
     Control *ctl;
     int grid_p;           // CTAs of primal_kernel (partials to read)
     double reflection;
+    int64_t hot;          // leading entries of y each primal CTA copies to shared memory
+    // panel path of A's long rows (nk_panel.cuh): partial[p * panel_rows + i]
+    const double *panel_partial;
+    int64_t panel_rows;
+    int npanels;
 };
 
 __device__ __forceinline__ double clampd(double v, double lo, double hi) {
@@ -153,19 +168,43 @@ __device__ __forceinline__ bool split_chunk(double *wpart /* this warp's 32 */, 
 // chunk combine.  Kept out of line so that the register budget of the kernels'
 // main path does not carry it.  init_vec (may be null) gives the row sum's
 // start; on true, *row and *total hold the completed row.
-template <class Acc, int G = 0, class V, class I, class X>
+template <class Acc, int G = 0, bool HOT = false, class V, class I, class X>
 __device__ __noinline__ bool split_lane(const Sell<V, I> M, int64_t vr, int len,
                                         const X *__restrict__ x, const double *init_vec,
-                                        double *wpart, int64_t *row, double *total) {
+                                        double *wpart, int64_t *row, double *total,
+                                        const X *hot = nullptr, int64_t nhot = 0) {
 #if NK_SPLIT_PIPE
     const double part = double(sell_dot_pipelined<Acc, kUnrollSplit>(M, vr, len, Acc(0), x));
 #else
-    const double part = double(sell_dot<Acc, kUnrollSplit, G>(M, vr, len, Acc(0), x));
+    const double part =
+        double(sell_dot<Acc, kUnrollSplit, G, HOT>(M, vr, len, Acc(0), x, hot, nhot));
 #endif
     const int4 sg = M.seg[vr];
     *row = sg.x;
     const double init = (sg.x >= 0 && init_vec) ? init_vec[sg.x] : 0.;
     return split_chunk(wpart, M.slots, M.counters, sg, vr, part, init, total);
+}
+
+// Copies `bytes` rounded up to 16 from global `src` to shared `dst` with the
+// CTA's T threads, 16-byte loads, four in flight per thread.  Both addresses
+// are 16-byte aligned; the rounding reads at most 15 bytes past the end of
+// `src`, which every device buffer of the engine carries as zeroed slack.
+template <int T>
+__device__ __forceinline__ void stage16(void *dst, const void *src, int64_t bytes) {
+    const int4 *s = static_cast<const int4 *>(src);
+    int4 *d = static_cast<int4 *>(dst);
+    const int64_t n16 = (bytes + 15) >> 4;
+    int64_t k = threadIdx.x;
+    for (; k + 3 * T < n16; k += 4 * T) {
+        const int4 a = __ldcg(s + k), b = __ldcg(s + k + T), c = __ldcg(s + k + 2 * T),
+                   e = __ldcg(s + k + 3 * T);
+        d[k] = a;
+        d[k + T] = b;
+        d[k + 2 * T] = c;
+        d[k + 3 * T] = e;
+    }
+    for (; k < n16; k += T)
+        d[k] = __ldcg(s + k);
 }
 
 // Index of the first SELL chunk of the calling warp and the warp stride of a
@@ -180,11 +219,17 @@ __device__ __forceinline__ int64_t chunk_stride() {
 // ------------------------------------------------------------------ primal
 // SPLIT: the matrix has split rows (kernels without them skip that path
 // entirely, which keeps their register footprint small).
-template <class Acc, class V, class I, bool SPARSE_Q, bool FP32G, bool SPLIT>
-__global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS)
+// HOT: the CTA first copies y[0, v.hot) (y32 with FP32 gathers) into dynamic
+// shared memory and gathers those entries from there.  Rows of A are in
+// engine order, longest first, so these are the rows with the most entries,
+// i.e. the y entries that the rows of A^T gather most often.
+template <class Acc, class V, class I, bool SPARSE_Q, bool FP32G, bool SPLIT, bool HOT>
+__global__ void __launch_bounds__(kFusedThreads, kFusedMinBlocks)
     primal_kernel(Sell<V, I> At, QCsr<V, I> Q, Vecs v) {
-    __shared__ double red[kWarps];
-    __shared__ double wpart[kWarps][32];
+    __shared__ double red[kFusedWarps];
+    __shared__ double wpart[kFusedWarps][32];
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    using Y = typename std::conditional<FP32G, float, double>::type;
     const Control &ctl = *v.ctl;
     double mine = 0;
     bool bad = false;
@@ -197,6 +242,16 @@ __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS)
         double *xt = cur ? v.x0 : v.x1;
         const double *y = cur ? v.y1 : v.y0;
         const float *y32 = cur ? v.y32_1 : v.y32_0;
+        Y *hot = reinterpret_cast<Y *>(dyn_smem);
+        if constexpr (HOT) {
+            const Y *ys;
+            if constexpr (FP32G)
+                ys = y32;
+            else
+                ys = y;
+            stage16<kFusedThreads>(hot, ys, v.hot * int64_t(sizeof(Y)));
+            __syncthreads();
+        }
         // epilogue of column j; g = c_j + (A^T y)_j
         auto finish = [&](int64_t j, double g, double xj, double qj, double lj, double uj,
                           double aj) {
@@ -233,9 +288,11 @@ __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS)
 #endif
                 double g;
                 if constexpr (FP32G)
-                    g = cj + double(sell_dot<Acc>(At, vr, len, Acc(0), y32));
+                    g = cj + double(sell_dot<Acc, kUnroll, 0, HOT>(At, vr, len, Acc(0), y32, hot,
+                                                                   v.hot));
                 else // FP64 accumulation starts from c_j, like the CPU loop (src/cpu.cpp:108-111)
-                    g = double(sell_dot<Acc>(At, vr, len, Acc(cj), y));
+                    g = double(sell_dot<Acc, kUnroll, 0, HOT>(At, vr, len, Acc(cj), y, hot,
+                                                              v.hot));
 #if NK_PREFETCH
                 finish(j, g, xj, qj, lj, uj, aj);
 #else
@@ -246,9 +303,11 @@ __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS)
                 double g;
                 bool done;
                 if constexpr (FP32G) // FP32 sums add c_j afterwards, in FP64
-                    done = split_lane<Acc>(At, vr, len, y32, nullptr, wpart[threadIdx.x >> 5], &j, &g);
+                    done = split_lane<Acc, 0, HOT>(At, vr, len, y32, nullptr,
+                                                   wpart[threadIdx.x >> 5], &j, &g, hot, v.hot);
                 else
-                    done = split_lane<Acc>(At, vr, len, y, v.c, wpart[threadIdx.x >> 5], &j, &g);
+                    done = split_lane<Acc, 0, HOT>(At, vr, len, y, v.c, wpart[threadIdx.x >> 5],
+                                                   &j, &g, hot, v.hot);
                 if (done) {
                     if constexpr (FP32G)
                         g = v.c[j] + g;
@@ -258,7 +317,7 @@ __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS)
         }
     }
     double tot[1] = {bad ? INFINITY : mine};
-    cta_sum<1>(tot, red);
+    cta_sum<1, kFusedWarps>(tot, red);
     if (threadIdx.x == 0)
         v.part_p[blockIdx.x] = tot[0];
 }
@@ -313,10 +372,15 @@ __device__ inline void decide(Vecs &v, double p, double d, double c) {
         s.rejected += 1;
 }
 
-template <class Acc, class V, class I, bool FP32G, bool SPLIT>
-__global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS) dual_kernel(Sell<V, I> A, Vecs v) {
-    __shared__ double red[kWarps * 3];
-    __shared__ double wpart[kWarps][32];
+// PANEL: A's long rows (engine rows [0, v.panel_rows)) come from panel_kernel
+// as one partial sum per column panel; the warp schedule lists them as
+// "combine chunks" (encoded -k-1 for rows [32k, 32k+32)) in place of their
+// split-row chunks, and a lane adds its row's partials in panel order.
+template <class Acc, class V, class I, bool FP32G, bool SPLIT, bool PANEL = false>
+__global__ void __launch_bounds__(kFusedThreads, kFusedMinBlocks)
+    dual_kernel(Sell<V, I> A, Vecs v) {
+    __shared__ double red[kFusedWarps * 3];
+    __shared__ double wpart[kFusedWarps][32];
     __shared__ bool last;
     const Control &ctl = *v.ctl;
     double dy2 = 0, cpl = 0;
@@ -350,6 +414,32 @@ __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS) dual_kernel(Sell<V, I
         const int lane = threadIdx.x & 31;
         WarpChunks<V, I> chunks(A);
         for (int64_t ch; chunks.next(&ch);) {
+            if constexpr (PANEL) {
+                if (ch < 0) { // a long row: its panel partials, in panel order
+                    const int64_t i = (-ch - 1) * 32 + lane;
+                    if (i >= v.panel_rows)
+                        continue;
+                    const double yi = y[i], axi = ax[i], rli = v.rl[i], rui = v.ru[i];
+                    const double ai = pending ? v.ya[i] : 0.;
+                    const double *pp = v.panel_partial + i;
+                    const int64_t stride = v.panel_rows;
+                    double delta = 0;
+                    int p = 0;
+                    for (; p + 4 <= v.npanels; p += 4) {
+                        const double a0 = __ldcg(pp + p * stride), a1 = __ldcg(pp + (p + 1) * stride),
+                                     a2 = __ldcg(pp + (p + 2) * stride),
+                                     a3 = __ldcg(pp + (p + 3) * stride);
+                        delta += a0;
+                        delta += a1;
+                        delta += a2;
+                        delta += a3;
+                    }
+                    for (; p < v.npanels; ++p)
+                        delta += __ldcg(pp + p * stride);
+                    finish(i, delta, yi, axi, rli, rui, ai);
+                    continue;
+                }
+            }
             const int64_t vr = ch * 32 + lane;
             if (vr >= A.nv)
                 continue;
@@ -384,7 +474,7 @@ __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS) dual_kernel(Sell<V, I
         }
     }
     double tot[2] = {bad ? INFINITY : dy2, cpl};
-    cta_sum<2>(tot, red);
+    cta_sum<2, kFusedWarps>(tot, red);
     if (threadIdx.x == 0) {
         v.part_d[2 * blockIdx.x] = tot[0];
         v.part_d[2 * blockIdx.x + 1] = tot[1];
@@ -399,14 +489,14 @@ __global__ void __launch_bounds__(kThreads, NK_MIN_BLOCKS) dual_kernel(Sell<V, I
     // complete; combine partials in index order (deterministic) and decide.
     __threadfence();
     double p = 0, d = 0, c = 0;
-    for (int b = threadIdx.x; b < v.grid_p; b += kThreads)
+    for (int b = threadIdx.x; b < v.grid_p; b += kFusedThreads)
         p += v.part_p[b];
-    for (int b = threadIdx.x; b < int(gridDim.x); b += kThreads) {
+    for (int b = threadIdx.x; b < int(gridDim.x); b += kFusedThreads) {
         d += v.part_d[2 * b];
         c += v.part_d[2 * b + 1];
     }
     double r3[3] = {p, d, c};
-    cta_sum<3>(r3, red);
+    cta_sum<3, kFusedWarps>(r3, red);
     if (threadIdx.x == 0) {
         decide(v, r3[0], r3[1], r3[2]);
         v.ctl->arrive = 0;

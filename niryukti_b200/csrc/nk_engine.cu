@@ -9,6 +9,7 @@
 // and out, so callers only ever see their own order.
 #include "nk_common.cuh"
 #include "nk_device.cuh"
+#include "nk_panel.cuh"
 #include "nk_host.hpp"
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
@@ -131,6 +132,40 @@ struct QMatrix {
     }
     size_t device_bytes() const {
         return ptr.bytes() + idx64.bytes() + idx32.bytes() + val64.bytes() + val32.bytes();
+    }
+};
+
+// A's long rows by column panel (nk_panel.cuh), for the dual kernel's A dx.
+struct PanelMatrix {
+    int64_t rows = 0, cols = 0, width = 0, entries = 0, padded = 0;
+    int npanels = 0, vbits = 64, grid = 0;
+    size_t smem = 0; // dynamic shared memory of panel_kernel: one dx slice
+    DevBuf<int64_t> uoff, cptr;
+    DevBuf<int4> units;
+    DevBuf<int2> lane;
+    DevBuf<uint16_t> lidx;
+    DevBuf<double> val64, partial;
+    DevBuf<float> val32;
+    template <class V> PanelView<V> view() const {
+        PanelView<V> P;
+        P.rows = rows;
+        P.cols = cols;
+        P.width = width;
+        P.uoff = uoff.p;
+        P.units = units.p;
+        P.cptr = cptr.p;
+        P.lane = lane.p;
+        P.lidx = lidx.p;
+        if constexpr (sizeof(V) == 8)
+            P.val = reinterpret_cast<const V *>(val64.p);
+        else
+            P.val = reinterpret_cast<const V *>(val32.p);
+        P.partial = partial.p;
+        return P;
+    }
+    size_t device_bytes() const {
+        return uoff.bytes() + cptr.bytes() + units.bytes() + lane.bytes() + lidx.bytes() +
+               val64.bytes() + partial.bytes() + val32.bytes();
     }
 };
 
@@ -401,6 +436,26 @@ void upload_raw(const nk_csr *H, int vbits, cudaStream_t stream, DevBuf<int64_t>
     cuda_check(cudaStreamSynchronize(stream), "matrix upload");
 }
 
+// The primal kernel instance for a model: sparse Q or not, split rows of A^T
+// or not, staged y entries or not (each leaves unused paths out of the build).
+template <class V, class I> using PrimalFn = void (*)(Sell<V, I>, QCsr<V, I>, Vecs);
+template <class Acc, class V, class I>
+PrimalFn<V, I> primal_kernel_for(bool sparse_q, bool split, bool hot) {
+    constexpr bool F = sizeof(Acc) == 4;
+    if (sparse_q) {
+        if (split)
+            return hot ? primal_kernel<Acc, V, I, true, F, true, true>
+                       : primal_kernel<Acc, V, I, true, F, true, false>;
+        return hot ? primal_kernel<Acc, V, I, true, F, false, true>
+                   : primal_kernel<Acc, V, I, true, F, false, false>;
+    }
+    if (split)
+        return hot ? primal_kernel<Acc, V, I, false, F, true, true>
+                   : primal_kernel<Acc, V, I, false, F, true, false>;
+    return hot ? primal_kernel<Acc, V, I, false, F, false, true>
+               : primal_kernel<Acc, V, I, false, F, false, false>;
+}
+
 // ------------------------------------------------------------------ engine
 struct Engine {
     int64_t n = 0, m = 0;
@@ -412,6 +467,8 @@ struct Engine {
     cudaStream_t stream = nullptr;
     SellMatrix A, At;
     QMatrix Q;
+    PanelMatrix pan; // A's long rows by column panel (the dual SpMV), when panels
+    bool panels = false;
     DevBuf<double> c, q, lb, ub, rl, ru, x[2], y[2], ax[2], xa, ya, dx, anchor_x, anchor_y,
         anchor_ax, part_p, part_d, mon_ax, mon_aty, mon_qx, mon_part, mon_out;
     DevBuf<float> dx32, y32[2];
@@ -419,6 +476,8 @@ struct Engine {
     DevBuf<unsigned> mon_arrive;
     Control *host_ctl = nullptr; // pinned mirror
     int grid_p = 1, grid_d = 1, grid_s = 148;
+    int64_t hot = 0;      // leading y entries the primal kernel stages in shared memory
+    size_t hot_bytes = 0; // its dynamic shared memory per CTA
     int64_t accepted = 0, rejected = 0, trials = 0;
     int empty_chunks = 0;
     bool request_restart = false;
@@ -472,6 +531,10 @@ struct Engine {
         v.ctl = ctl.p;
         v.grid_p = grid_p;
         v.reflection = reflection;
+        v.hot = hot;
+        v.panel_partial = pan.partial.p;
+        v.panel_rows = panels ? pan.rows : 0;
+        v.npanels = panels ? pan.npanels : 0;
         return v;
     }
 
@@ -484,21 +547,26 @@ struct Engine {
         auto qm = Q.view<V, I>();
         if (ev[0])
             cudaEventRecord(ev[0], stream);
-        const bool ps = At.nsv > 0, ds = A.nsv > 0;
-        if (sparse_q && ps)
-            primal_kernel<Acc, V, I, true, F32, true><<<grid_p, kThreads, 0, stream>>>(at, qm, v);
-        else if (sparse_q)
-            primal_kernel<Acc, V, I, true, F32, false><<<grid_p, kThreads, 0, stream>>>(at, qm, v);
-        else if (ps)
-            primal_kernel<Acc, V, I, false, F32, true><<<grid_p, kThreads, 0, stream>>>(at, qm, v);
-        else
-            primal_kernel<Acc, V, I, false, F32, false><<<grid_p, kThreads, 0, stream>>>(at, qm, v);
+        primal_kernel_for<Acc, V, I>(sparse_q, At.nsv > 0, hot > 0)<<<grid_p, kFusedThreads,
+                                                                       hot_bytes, stream>>>(at, qm, v);
         if (ev[1])
             cudaEventRecord(ev[1], stream);
-        if (ds)
-            dual_kernel<Acc, V, I, F32, true><<<grid_d, kThreads, 0, stream>>>(a, v);
+        if (panels) {
+            using X = typename std::conditional<F32, float, double>::type;
+            const X *dxp;
+            if constexpr (F32)
+                dxp = dx32.p;
+            else
+                dxp = dx.p;
+            panel_kernel<Acc, V, X><<<pan.grid, kPanelThreads, pan.smem, stream>>>(
+                pan.view<V>(), dxp, ctl.p);
+            if (ev[3])
+                cudaEventRecord(ev[3], stream);
+            dual_kernel<Acc, V, I, F32, false, true><<<grid_d, kFusedThreads, 0, stream>>>(a, v);
+        } else if (A.nsv > 0)
+            dual_kernel<Acc, V, I, F32, true><<<grid_d, kFusedThreads, 0, stream>>>(a, v);
         else
-            dual_kernel<Acc, V, I, F32, false><<<grid_d, kThreads, 0, stream>>>(a, v);
+            dual_kernel<Acc, V, I, F32, false><<<grid_d, kFusedThreads, 0, stream>>>(a, v);
         if (ev[2])
             cudaEventRecord(ev[2], stream);
         if (halpern)
@@ -907,8 +975,11 @@ struct Engine {
     }
 
     // Runs `count` trials one by one with events around each kernel; returns the
-    // mean primal and dual kernel durations in milliseconds.
-    void profile(int count, double tau, double sigma, double *ms_primal, double *ms_dual) {
+    // mean durations in milliseconds of the primal kernel, of the dual step (the
+    // panel kernel, when A has panels, plus the dual kernel) and of the panel
+    // kernel alone (0 without panels).
+    void profile(int count, double tau, double sigma, double *ms_primal, double *ms_dual,
+                 double *ms_panel = nullptr) {
         if (count <= 0)
             throw Error(NK_ERR_INVALID, "profile needs a positive trial count");
         sync_ctl();
@@ -917,16 +988,19 @@ struct Engine {
         push_ctl();
         for (auto &e : ev)
             cuda_check(cudaEventCreate(&e), "event");
-        double tp = 0, td = 0;
+        double tp = 0, td = 0, tk = 0;
         try {
             for (int t = 0; t < count; ++t) {
                 launch_trial();
                 cuda_check(cudaEventSynchronize(ev[2]), "profile sync");
-                float a = 0, b = 0;
+                float a = 0, b = 0, k = 0;
                 cudaEventElapsedTime(&a, ev[0], ev[1]);
                 cudaEventElapsedTime(&b, ev[1], ev[2]);
+                if (panels)
+                    cudaEventElapsedTime(&k, ev[1], ev[3]);
                 tp += a;
                 td += b;
+                tk += k;
             }
         } catch (...) {
             for (auto &e : ev) {
@@ -945,6 +1019,8 @@ struct Engine {
         rejected = int64_t(host_ctl->rejected);
         *ms_primal = tp / count;
         *ms_dual = td / count;
+        if (ms_panel)
+            *ms_panel = tk / count;
     }
 
     // Mean duration (ms) of `reps` plain SpMVs with A (which = 0: A x into Ax) or
@@ -979,7 +1055,7 @@ struct Engine {
     }
 
     size_t device_bytes() const {
-        size_t b = A.device_bytes() + At.device_bytes() + Q.device_bytes();
+        size_t b = A.device_bytes() + At.device_bytes() + Q.device_bytes() + pan.device_bytes();
         for (auto *d : {&c, &q, &lb, &ub, &rl, &ru, &x[0], &x[1], &y[0], &y[1], &ax[0], &ax[1],
                         &xa, &ya, &dx, &anchor_x, &anchor_y, &anchor_ax, &part_p, &part_d,
                         &scratch_n, &scratch_m})
@@ -989,7 +1065,7 @@ struct Engine {
     }
 };
 
-// Balanced warp schedule for a persistent grid of `warps` warps (kWarps per
+// Balanced warp schedule for a persistent grid of `warps` warps (cta_warps per
 // CTA, all CTAs resident at once: occupancy_grid never launches more).
 //
 // Two costs per chunk of padded length L:
@@ -1008,109 +1084,341 @@ struct Engine {
 // warps, hence on a subset of the SMs, which then set the kernel's time.
 // Which warp runs a chunk changes no row sum, and the per-CTA partial sums are
 // fixed for a given schedule, so results stay deterministic.
-void build_schedule(SellMatrix &M, int64_t warps, cudaStream_t s) {
-    const int64_t nch = int64_t(M.chunk_len.size());
-    const int64_t ctas = std::max<int64_t>(1, warps / kWarps);
-    warps = ctas * kWarps;
-    const int64_t split_chunks = M.nsv / 32;
-    std::vector<int64_t> work(static_cast<size_t>(nch)), chain(static_cast<size_t>(nch));
-    for (int64_t c = 0; c < nch; ++c) {
-        const int64_t L = M.chunk_len[size_t(c)];
-        const bool split = c < split_chunks;
-        const int64_t u = split ? kUnrollSplit : kUnroll;
-        work[size_t(c)] = 44 * L + (split ? 100 : 70);
-        chain[size_t(c)] = (split && NK_SPLIT_PIPE ? (L + u - 1) / u + 1 : 2 * (L / u) + 2 * (L % u)) +
-                           (split ? 6 : 4);
-    }
+
+// Longest-first list scheduling: items (by index into cost) go, costliest
+// first, to the least-loaded machine (ties to the lowest index); owner[k] is
+// item k's machine.  Returns the items in assignment order.
+std::vector<int64_t> lpt_assign(const std::vector<int64_t> &items, const std::vector<int64_t> &cost,
+                                int64_t machines, std::vector<int64_t> &owner) {
     using Slot = std::pair<int64_t, int64_t>; // (load so far, machine)
-    auto lpt = [](const std::vector<int64_t> &items, const std::vector<int64_t> &cost,
-                  int64_t machines, std::vector<int64_t> &owner) {
-        std::vector<int64_t> order(items);
-        std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
-            return cost[size_t(a)] > cost[size_t(b)];
-        });
-        std::priority_queue<Slot, std::vector<Slot>, std::greater<Slot>> heap;
-        for (int64_t k = 0; k < machines; ++k)
-            heap.push({0, k});
-        for (int64_t c : order) {
-            Slot t = heap.top();
-            heap.pop();
-            owner[size_t(c)] = t.second;
-            heap.push({t.first + cost[size_t(c)], t.second});
-        }
-        return order; // assignment order, costliest first
-    };
-    std::vector<int64_t> all(static_cast<size_t>(nch)), cta(static_cast<size_t>(nch));
-    for (int64_t c = 0; c < nch; ++c)
-        all[size_t(c)] = c;
-    lpt(all, work, ctas, cta);
-    // chunks of each CTA, then its warps
+    std::vector<int64_t> order(items);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int64_t a, int64_t b) { return cost[size_t(a)] > cost[size_t(b)]; });
+    std::priority_queue<Slot, std::vector<Slot>, std::greater<Slot>> heap;
+    for (int64_t k = 0; k < machines; ++k)
+        heap.push({0, k});
+    for (int64_t c : order) {
+        Slot t = heap.top();
+        heap.pop();
+        owner[size_t(c)] = t.second;
+        heap.push({t.first + cost[size_t(c)], t.second});
+    }
+    return order;
+}
+
+// The two-level schedule of `ids` (item k is ids[k], with memory work work[k]
+// and chain length chain[k]) onto `warps` persistent warps in CTAs of
+// cta_warps; uploads each warp's list (woff, wlist).
+void schedule_items(const std::vector<int64_t> &ids, const std::vector<int64_t> &work,
+                    const std::vector<int64_t> &chain, int64_t warps, int cta_warps,
+                    DevBuf<int64_t> &woff, DevBuf<int64_t> &wlist, cudaStream_t s) {
+    const int64_t nit = int64_t(ids.size());
+    const int64_t ctas = std::max<int64_t>(1, warps / cta_warps);
+    warps = ctas * cta_warps;
+    std::vector<int64_t> all(static_cast<size_t>(nit)), cta(static_cast<size_t>(nit));
+    for (int64_t k = 0; k < nit; ++k)
+        all[size_t(k)] = k;
+    lpt_assign(all, work, ctas, cta);
+    // items of each CTA, then its warps
     std::vector<int64_t> cstart(static_cast<size_t>(ctas + 1), 0);
-    for (int64_t c = 0; c < nch; ++c)
-        ++cstart[size_t(cta[size_t(c)] + 1)];
+    for (int64_t k = 0; k < nit; ++k)
+        ++cstart[size_t(cta[size_t(k)] + 1)];
     for (int64_t b = 0; b < ctas; ++b)
         cstart[size_t(b + 1)] += cstart[size_t(b)];
-    std::vector<int64_t> bychunk(static_cast<size_t>(std::max<int64_t>(1, nch)));
+    std::vector<int64_t> byitem(static_cast<size_t>(std::max<int64_t>(1, nit)));
     {
         std::vector<int64_t> pos(cstart.begin(), cstart.end() - 1);
-        for (int64_t c = 0; c < nch; ++c)
-            bychunk[size_t(pos[size_t(cta[size_t(c)])]++)] = c;
+        for (int64_t k = 0; k < nit; ++k)
+            byitem[size_t(pos[size_t(cta[size_t(k)])]++)] = k;
     }
     std::vector<int64_t> off(static_cast<size_t>(warps + 1), 0), seq;
-    seq.reserve(size_t(nch));
-    std::vector<int64_t> local_owner(static_cast<size_t>(nch));
-    std::vector<std::vector<int64_t>> lists(static_cast<size_t>(kWarps));
+    seq.reserve(size_t(nit));
+    std::vector<int64_t> local_owner(static_cast<size_t>(nit));
+    std::vector<std::vector<int64_t>> lists(static_cast<size_t>(cta_warps));
     for (int64_t b = 0; b < ctas; ++b) {
-        std::vector<int64_t> mine(bychunk.begin() + cstart[size_t(b)],
-                                  bychunk.begin() + cstart[size_t(b + 1)]);
+        std::vector<int64_t> mine(byitem.begin() + cstart[size_t(b)],
+                                  byitem.begin() + cstart[size_t(b + 1)]);
         for (auto &l : lists)
             l.clear();
-        for (int64_t c : lpt(mine, chain, kWarps, local_owner))
-            lists[size_t(local_owner[size_t(c)])].push_back(c);
-        for (int k = 0; k < kWarps; ++k) {
-            off[size_t(b * kWarps + k + 1)] = int64_t(lists[size_t(k)].size());
-            seq.insert(seq.end(), lists[size_t(k)].begin(), lists[size_t(k)].end());
+        for (int64_t k : lpt_assign(mine, chain, cta_warps, local_owner))
+            lists[size_t(local_owner[size_t(k)])].push_back(k);
+        for (int w = 0; w < cta_warps; ++w) {
+            off[size_t(b * cta_warps + w + 1)] = int64_t(lists[size_t(w)].size());
+            for (int64_t k : lists[size_t(w)])
+                seq.push_back(ids[size_t(k)]);
         }
     }
     for (int64_t w = 0; w < warps; ++w)
         off[size_t(w + 1)] += off[size_t(w)];
-    // every chunk exactly once
-    std::vector<char> seen(static_cast<size_t>(nch), 0);
-    for (int64_t c : seq)
-        if (c < 0 || c >= nch || seen[size_t(c)]++)
-            throw Error(NK_ERR_INVALID, "internal: warp schedule is not a permutation");
-    if (int64_t(seq.size()) != nch || off[size_t(warps)] != nch)
+    if (int64_t(seq.size()) != nit || off[size_t(warps)] != nit)
         throw Error(NK_ERR_INVALID, "internal: warp schedule size");
+    {   // every item exactly once
+        std::vector<int64_t> got(seq), want(ids);
+        std::sort(got.begin(), got.end());
+        std::sort(want.begin(), want.end());
+        if (got != want)
+            throw Error(NK_ERR_INVALID, "internal: warp schedule is not a permutation");
+    }
     if (seq.empty())
         seq.push_back(0);
-    upload_vector(M.woff, off, s);
-    upload_vector(M.wlist, seq, s);
+    upload_vector(woff, off, s);
+    upload_vector(wlist, seq, s);
+}
+
+// Memory work and chain length of a SELL chunk of padded length L (see above).
+void chunk_costs(int64_t L, bool split, int64_t *work, int64_t *chain) {
+    const int64_t u = split ? kUnrollSplit : kUnroll;
+    *work = 44 * L + (split ? 100 : 70);
+    *chain = (split && NK_SPLIT_PIPE ? (L + u - 1) / u + 1 : 2 * (L / u) + 2 * (L % u)) +
+             (split ? 6 : 4);
+}
+
+void build_schedule(SellMatrix &M, int64_t warps, int cta_warps, cudaStream_t s) {
+    const int64_t nch = int64_t(M.chunk_len.size());
+    const int64_t split_chunks = M.nsv / 32;
+    std::vector<int64_t> ids(static_cast<size_t>(nch)), work(ids.size()), chain(ids.size());
+    for (int64_t c = 0; c < nch; ++c) {
+        ids[size_t(c)] = c;
+        chunk_costs(M.chunk_len[size_t(c)], c < split_chunks, &work[size_t(c)], &chain[size_t(c)]);
+    }
+    schedule_items(ids, work, chain, warps, cta_warps, M.woff, M.wlist, s);
+}
+
+// The dual kernel's schedule when A's long rows take the panel path: the
+// chunks past the split region, plus one combine chunk per 32 long rows
+// (encoded -k-1), whose lanes each read `npanels` partials (8 sectors per
+// panel for the warp) and run the row epilogue.
+void build_dual_panel_schedule(SellMatrix &M, int64_t long_rows, int npanels, int64_t warps,
+                               int cta_warps, cudaStream_t s) {
+    const int64_t nch = int64_t(M.chunk_len.size());
+    const int64_t split_chunks = M.nsv / 32;
+    const int64_t combine = (long_rows + 31) / 32;
+    std::vector<int64_t> ids, work, chain;
+    for (int64_t k = 0; k < combine; ++k) {
+        ids.push_back(-k - 1);
+        work.push_back(8 * int64_t(npanels) + 70);
+        chain.push_back(npanels / 4 + 4);
+    }
+    for (int64_t c = split_chunks; c < nch; ++c) {
+        int64_t w = 0, ch = 0;
+        chunk_costs(M.chunk_len[size_t(c)], false, &w, &ch);
+        ids.push_back(c);
+        work.push_back(w);
+        chain.push_back(ch);
+    }
+    schedule_items(ids, work, chain, warps, cta_warps, M.woff, M.wlist, s);
 }
 
 // Persistent grid: as many CTAs as fit on the device at once, at most one warp
 // per SELL chunk.
-int occupancy_grid(const void *kernel, int64_t chunks) {
+int occupancy_grid(const void *kernel, int64_t chunks, int threads = kThreads, size_t dyn = 0) {
     int dev = 0, sms = 148, per = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kThreads, 0),
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, dyn),
                "occupancy");
     per = std::max(1, per);
-    int64_t need = (chunks + kWarps - 1) / kWarps;
+    int64_t need = (chunks + threads / 32 - 1) / (threads / 32);
     return int(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sms) * per)));
+}
+
+// Shared memory a CTA of `kernel` can use dynamically while the SM still holds
+// ctas_per_sm of them: the SM's shared memory split between them, less the
+// per-CTA reservation and the kernel's static arrays (for the primal kernel's
+// staged y entries and the panel kernel's dx slice).
+size_t smem_budget(const void *kernel, int ctas_per_sm) {
+    int dev = 0, per_sm = 0, optin = 0, reserved = 0;
+    cudaGetDevice(&dev);
+    cuda_check(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev),
+               "shared memory per SM");
+    cuda_check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev),
+               "shared memory per block");
+    cuda_check(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev),
+               "reserved shared memory");
+    cudaFuncAttributes fa{};
+    cuda_check(cudaFuncGetAttributes(&fa, kernel), "kernel attributes");
+    int64_t b = int64_t(per_sm) / ctas_per_sm - reserved - int64_t(fa.sharedSizeBytes);
+    b = std::min<int64_t>(b, int64_t(optin) - int64_t(fa.sharedSizeBytes));
+    return size_t(std::max<int64_t>(0, b) & ~int64_t(15));
+}
+size_t hot_budget(const void *kernel) {
+    size_t b = smem_budget(kernel, kFusedMinBlocks);
+#ifdef NK_HOT_MAX_BYTES
+    b = std::min<size_t>(b, size_t(NK_HOT_MAX_BYTES));
+#endif
+    return b;
+}
+
+// The panel kernel instance of a precision, with its dynamic shared memory
+// raised to `bytes`; returns the kernel and the budget it allows.
+const void *panel_kernel_for(int precision) {
+    if (precision == NK_PRECISION_FP64)
+        return (const void *)panel_kernel<double, double, double>;
+    if (precision == NK_PRECISION_MIXED)
+        return (const void *)panel_kernel<double, float, double>;
+    return (const void *)panel_kernel<float, float, float>;
+}
+
+// Panel layout (nk_panel.cuh) of the first `rows` rows of an engine-order CSR
+// (host ptr; device int64 indices and double values), panels of `width`
+// columns, work units spread over `grid` CTAs.  Built on the host from one
+// download of those rows' entries.
+void build_panels(PanelMatrix &P, int64_t rows, int64_t cols, const std::vector<int64_t> &ptr,
+                  const int64_t *didx, const double *dval, int64_t width, int vbits, int grid,
+                  size_t xsize, cudaStream_t s) {
+    P.rows = rows;
+    P.cols = cols;
+    P.width = width;
+    P.vbits = vbits;
+    P.grid = grid;
+    const int64_t E = ptr[size_t(rows)];
+    P.entries = E;
+    const int64_t np = (cols + width - 1) / width;
+    P.npanels = int(np);
+    std::vector<int64_t> hidx(static_cast<size_t>(E));
+    std::vector<double> hval(static_cast<size_t>(E));
+    if (E) {
+        cuda_check(cudaMemcpyAsync(hidx.data(), didx, size_t(E) * 8, cudaMemcpyDeviceToHost, s),
+                   "panel index download");
+        cuda_check(cudaMemcpyAsync(hval.data(), dval, size_t(E) * 8, cudaMemcpyDeviceToHost, s),
+                   "panel value download");
+        cuda_check(cudaStreamSynchronize(s), "panel download");
+    }
+    // entries of each (panel, row)
+    std::vector<int32_t> cnt(size_t(np * rows), 0);
+    for (int64_t r = 0; r < rows; ++r)
+        for (int64_t k = ptr[size_t(r)]; k < ptr[size_t(r + 1)]; ++k)
+            ++cnt[size_t((hidx[size_t(k)] / width) * rows + r)];
+    // per panel: its rows with entries, most entries first (stable), in chunks of 32
+    std::vector<int32_t> rank(size_t(np * rows), -1);
+    std::vector<int64_t> first_chunk(size_t(np + 1), 0), cptr(1, 0);
+    std::vector<int2> lanes;
+    std::vector<int64_t> chunk_panel;
+    std::vector<int64_t> list;
+    for (int64_t p = 0; p < np; ++p) {
+        const int32_t *cp = cnt.data() + p * rows;
+        list.clear();
+        for (int64_t r = 0; r < rows; ++r)
+            if (cp[r] > 0)
+                list.push_back(r);
+        std::stable_sort(list.begin(), list.end(),
+                         [&](int64_t a, int64_t b) { return cp[a] > cp[b]; });
+        for (size_t q = 0; q < list.size(); ++q)
+            rank[size_t(p * rows + list[q])] = int32_t(q);
+        const int64_t nch = (int64_t(list.size()) + 31) / 32;
+        for (int64_t c = 0; c < nch; ++c) {
+            int32_t top = 0;
+            for (int t = 0; t < 32; ++t) {
+                const size_t q = size_t(c * 32 + t);
+                if (q < list.size()) {
+                    lanes.push_back(make_int2(int(list[q]), cp[list[q]]));
+                    top = std::max(top, cp[list[q]]);
+                } else
+                    lanes.push_back(make_int2(-1, 0));
+            }
+            cptr.push_back(cptr.back() + 32 * int64_t(top));
+            chunk_panel.push_back(p);
+        }
+        first_chunk[size_t(p + 1)] = first_chunk[size_t(p)] + nch;
+    }
+    const int64_t nchunks = first_chunk[size_t(np)];
+    P.padded = cptr.back();
+    std::vector<uint16_t> hl(static_cast<size_t>(std::max<int64_t>(1, P.padded)), 0);
+    std::vector<double> hv64(vbits == 64 ? size_t(std::max<int64_t>(1, P.padded)) : 1, 0.);
+    std::vector<float> hv32(vbits == 64 ? 1 : size_t(std::max<int64_t>(1, P.padded)), 0.f);
+    std::vector<int32_t> &fill = cnt; // reused: entries placed so far per (panel, row)
+    std::fill(fill.begin(), fill.end(), 0);
+    for (int64_t r = 0; r < rows; ++r)
+        for (int64_t k = ptr[size_t(r)]; k < ptr[size_t(r + 1)]; ++k) {
+            const int64_t j = hidx[size_t(k)], p = j / width;
+            const int64_t q = rank[size_t(p * rows + r)];
+            const int64_t c = first_chunk[size_t(p)] + q / 32;
+            const int64_t at = cptr[size_t(c)] + 32 * int64_t(fill[size_t(p * rows + r)]++) + q % 32;
+            hl[size_t(at)] = uint16_t(j - p * width);
+            if (vbits == 64)
+                hv64[size_t(at)] = hval[size_t(k)];
+            else
+                hv32[size_t(at)] = float(hval[size_t(k)]);
+        }
+    // work units: runs of one panel's chunks, about two per CTA; cost in bytes
+    // (index and value stream, lane records, partial writes) plus half the
+    // slice copy, which comes from L2
+    const int64_t vsize = vbits / 8;
+    std::vector<int64_t> ccost(static_cast<size_t>(nchunks));
+    int64_t total = 0;
+    for (int64_t c = 0; c < nchunks; ++c) {
+        ccost[size_t(c)] = (cptr[size_t(c + 1)] - cptr[size_t(c)]) * (2 + vsize) + 32 * 16;
+        total += ccost[size_t(c)];
+    }
+    const int64_t target = std::max<int64_t>(1, total / std::max<int64_t>(1, 2 * int64_t(grid)));
+    std::vector<int4> units;
+    std::vector<int64_t> ucost;
+    for (int64_t p = 0; p < np; ++p) {
+        const int64_t cols_p = std::min(width, cols - p * width);
+        int64_t c = first_chunk[size_t(p)];
+        while (c < first_chunk[size_t(p + 1)]) {
+            int64_t e = c, w = 0;
+            while (e < first_chunk[size_t(p + 1)] && (e == c || w + ccost[size_t(e)] <= target))
+                w += ccost[size_t(e++)];
+            units.push_back(make_int4(int(p), int(c), int(e), 0));
+            ucost.push_back(w + cols_p * int64_t(xsize) / 2);
+            c = e;
+        }
+    }
+    const int64_t nunits = int64_t(units.size());
+    std::vector<int64_t> ids(static_cast<size_t>(nunits)), owner(static_cast<size_t>(nunits));
+    std::iota(ids.begin(), ids.end(), 0);
+    lpt_assign(ids, ucost, grid, owner);
+    std::vector<int64_t> uoff(size_t(grid + 1), 0);
+    for (int64_t u = 0; u < nunits; ++u)
+        ++uoff[size_t(owner[size_t(u)] + 1)];
+    for (int b = 0; b < grid; ++b)
+        uoff[size_t(b + 1)] += uoff[size_t(b)];
+    std::vector<int4> ordered(static_cast<size_t>(std::max<int64_t>(1, nunits)));
+    {
+        std::vector<int64_t> pos(uoff.begin(), uoff.end() - 1);
+        for (int64_t u = 0; u < nunits; ++u)
+            ordered[size_t(pos[size_t(owner[size_t(u)])]++)] = units[size_t(u)];
+    }
+    upload_vector(P.uoff, uoff, s);
+    upload_vector(P.units, ordered, s);
+    upload_vector(P.cptr, cptr, s);
+    if (lanes.empty())
+        lanes.push_back(make_int2(-1, 0));
+    upload_vector(P.lane, lanes, s);
+    upload_vector(P.lidx, hl, s);
+    if (vbits == 64)
+        upload_vector(P.val64, hv64, s);
+    else
+        upload_vector(P.val32, hv32, s);
+    P.partial.alloc(size_t(std::max<int64_t>(1, np * rows)));
+    cuda_check(cudaMemsetAsync(P.partial.p, 0, P.partial.bytes(), s), "panel partials");
+    cuda_check(cudaStreamSynchronize(s), "panel build");
 }
 
 template <class Acc, class V, class I> void configure(Engine &E) {
     constexpr bool F32 = sizeof(Acc) == 4;
-    const bool ps = E.At.nsv > 0, ds = E.A.nsv > 0;
-    const void *pk = E.sparse_q ? (ps ? (const void *)primal_kernel<Acc, V, I, true, F32, true>
-                                      : (const void *)primal_kernel<Acc, V, I, true, F32, false>)
-                                : (ps ? (const void *)primal_kernel<Acc, V, I, false, F32, true>
-                                      : (const void *)primal_kernel<Acc, V, I, false, F32, false>);
-    const void *dk = ds ? (const void *)dual_kernel<Acc, V, I, F32, true>
-                        : (const void *)dual_kernel<Acc, V, I, F32, false>;
-    E.grid_p = occupancy_grid(pk, (E.At.nv + 31) / 32);
-    E.grid_d = occupancy_grid(dk, (E.A.nv + 31) / 32);
+    const bool ds = E.A.nsv > 0;
+    E.hot = 0;
+    E.hot_bytes = 0;
+    if (NK_HOT && E.m > 0) {
+        const void *pk = (const void *)primal_kernel_for<Acc, V, I>(E.sparse_q, E.At.nsv > 0, true);
+        const size_t ysize = F32 ? sizeof(float) : sizeof(double);
+        E.hot = std::min<int64_t>(E.m, int64_t(hot_budget(pk) / ysize));
+        E.hot_bytes = size_t((E.hot * int64_t(ysize) + 15) & ~int64_t(15));
+        if (E.hot > 0)
+            cuda_check(cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            int(E.hot_bytes)),
+                       "primal shared memory");
+        else
+            E.hot_bytes = 0;
+    }
+    const void *pk = (const void *)primal_kernel_for<Acc, V, I>(E.sparse_q, E.At.nsv > 0, E.hot > 0);
+    const void *dk = E.panels ? (const void *)dual_kernel<Acc, V, I, F32, false, true>
+                     : ds     ? (const void *)dual_kernel<Acc, V, I, F32, true>
+                              : (const void *)dual_kernel<Acc, V, I, F32, false>;
+    E.grid_p = occupancy_grid(pk, (E.At.nv + 31) / 32, kFusedThreads, E.hot_bytes);
+    E.grid_d = occupancy_grid(dk, (E.A.nv + 31) / 32, kFusedThreads, 0);
     E.grid_s = occupancy_grid((const void *)spmv_kernel<V, I>, int64_t(1) << 40);
 }
 
@@ -1196,6 +1504,35 @@ Engine *create_engine(const nk_csr *Ah, const nk_csr *Qh, const double *hc, cons
         auto pptr = permute_device_csr(m, aptr, rp.p, ri.p, rv.p, rperm, E->row_perm.p, d_cinv.p,
                                        pi, pv, s);
         build_sell(E->A, m, n, pptr, pi.p, pv.p, E->wide, vbits, s);
+        // A's long rows (the SELL's split rows) also by column panel, for the dual
+        // kernel: panels as wide as one CTA's shared memory holds dx entries, at
+        // most 65536 columns (16-bit offsets), a multiple of 16
+        if (NK_PANEL && NK_BALANCED && E->A.nsr > 0 && n > 0) { // the combine chunks
+                                                                 // live in the schedule
+            const void *pk = panel_kernel_for(o->precision);
+            const int64_t xsize = o->precision == NK_PRECISION_FP32 ? 4 : 8;
+            int64_t width = std::min<int64_t>(65536, int64_t(smem_budget(pk, kPanelMinBlocks)) / xsize);
+            width = std::min<int64_t>(width, (n + 15) / 16 * 16) / 16 * 16;
+            const int64_t np = width > 0 ? (n + width - 1) / width : 0;
+            if (width >= 16 && np * E->A.nsr <= (int64_t(1) << 25)) {
+                const size_t smem = size_t(width * xsize);
+                cuda_check(cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                int(smem)),
+                           "panel shared memory");
+                int dev = 0, sms = 148, per = 0;
+                cuda_check(cudaGetDevice(&dev), "device");
+                cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+                cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, pk, kPanelThreads,
+                                                                         smem),
+                           "panel occupancy");
+                if (per > 0) {
+                    build_panels(E->pan, E->A.nsr, n, pptr, pi.p, pv.p, width, vbits, sms * per,
+                                 size_t(xsize), s);
+                    E->pan.smem = smem;
+                    E->panels = true;
+                }
+            }
+        }
     }
     {
         // rows of A^T (columns of A) in engine order; the transpose lists every
@@ -1315,8 +1652,12 @@ Engine *create_engine(const nk_csr *Ah, const nk_csr *Qh, const double *hc, cons
         E->wide ? configure<double, float, int64_t>(*E) : configure<double, float, int32_t>(*E);
     else
         E->wide ? configure<float, float, int64_t>(*E) : configure<float, float, int32_t>(*E);
-    build_schedule(E->At, int64_t(E->grid_p) * kWarps, s);
-    build_schedule(E->A, int64_t(E->grid_d) * kWarps, s);
+    build_schedule(E->At, int64_t(E->grid_p) * kFusedWarps, kFusedWarps, s);
+    if (E->panels)
+        build_dual_panel_schedule(E->A, E->pan.rows, E->pan.npanels,
+                                  int64_t(E->grid_d) * kFusedWarps, kFusedWarps, s);
+    else
+        build_schedule(E->A, int64_t(E->grid_d) * kFusedWarps, kFusedWarps, s);
     E->part_p.alloc(size_t(E->grid_p));
     E->part_d.alloc(size_t(2 * E->grid_d));
     E->ctl.alloc(1);
@@ -1601,6 +1942,33 @@ nk_status nk_pdhg_profile(nk_pdhg *h, int count, double tau, double sigma, doubl
         need(ms_primal, "output");
         need(ms_dual, "output");
         h->e->profile(count, tau, sigma, ms_primal, ms_dual);
+    });
+}
+nk_status nk_pdhg_profile_kernels(nk_pdhg *h, int count, double tau, double sigma,
+                                  double ms[3]) {
+    return guard([&] {
+        NK_HANDLE
+        need(ms, "output");
+        double p = 0, d = 0, k = 0;
+        h->e->profile(count, tau, sigma, &p, &d, &k);
+        ms[0] = p;
+        ms[1] = k;
+        ms[2] = d - k;
+    });
+}
+nk_status nk_pdhg_layout_info(nk_pdhg *h, int64_t *long_rows, int64_t *panel_width,
+                              int *panels, int *kernels_per_trial) {
+    return guard([&] {
+        NK_HANDLE
+        const auto &e = *h->e;
+        if (long_rows)
+            *long_rows = e.panels ? e.pan.rows : 0;
+        if (panel_width)
+            *panel_width = e.panels ? e.pan.width : 0;
+        if (panels)
+            *panels = e.panels ? e.pan.npanels : 0;
+        if (kernels_per_trial)
+            *kernels_per_trial = 2 + (e.panels ? 1 : 0) + (e.halpern ? 1 : 0);
     });
 }
 nk_status nk_pdhg_time_spmv(nk_pdhg *h, int which, int reps, double *ms) {

@@ -42,8 +42,10 @@ template <int G, class T> __device__ __forceinline__ T gather_as(const T *p) {
     }
 }
 
-// Deterministic CTA reduction of NV doubles (fixed tree); result in thread 0.
-template <int NV> __device__ __forceinline__ void cta_sum(double (&v)[NV], double *smem /* kWarps*NV */) {
+// Deterministic CTA reduction of NV doubles (fixed tree) over a CTA of W
+// warps; result in thread 0.
+template <int NV, int W = kWarps>
+__device__ __forceinline__ void cta_sum(double (&v)[NV], double *smem /* W*NV */) {
 #pragma unroll
     for (int t = 0; t < NV; ++t)
 #pragma unroll
@@ -60,7 +62,7 @@ template <int NV> __device__ __forceinline__ void cta_sum(double (&v)[NV], doubl
 #pragma unroll
         for (int t = 0; t < NV; ++t) {
             double s = 0;
-            for (int i = 0; i < kWarps; ++i)
+            for (int i = 0; i < W; ++i)
                 s += smem[i * NV + t];
             v[t] = s;
         }

@@ -74,6 +74,9 @@ def library() -> C.CDLL:
     L.nk_pdhg_restore.argtypes = [C.c_void_p, _D, _I, C.c_int]
     L.nk_pdhg_stats.argtypes = [C.c_void_p, _I, _I]
     L.nk_pdhg_profile.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, _D, _D]
+    L.nk_pdhg_profile_kernels.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, _D]
+    L.nk_pdhg_layout_info.argtypes = [C.c_void_p, _I, _I, C.POINTER(C.c_int),
+                                      C.POINTER(C.c_int)]
     L.nk_pdhg_schedule_info.argtypes = [C.c_void_p, C.POINTER(C.c_int), _I, C.POINTER(C.c_int),
                                         _I, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.nk_pdhg_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
@@ -305,6 +308,24 @@ class PdhgBackend:
         check(self._L.nk_pdhg_profile(self._h, int(count), float(tau), float(sigma),
                                       C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    def profile_kernels(self, count: int, tau: float, sigma: float):
+        """Mean (primal, panel, dual) kernel durations in ms over `count` single
+        trials (panel 0 when A's long rows are not stored by column panel)."""
+        ms = np.zeros(3)
+        check(self._L.nk_pdhg_profile_kernels(self._h, int(count), float(tau), float(sigma),
+                                              _d(ms)))
+        return tuple(float(v) for v in ms)
+
+    def layout_info(self):
+        """The dual SpMV's layout: long rows stored by column panel, the panel
+        width, the panel count and the kernel launches per trial."""
+        r, w = C.c_int64(), C.c_int64()
+        p, k = C.c_int(), C.c_int()
+        check(self._L.nk_pdhg_layout_info(self._h, C.byref(r), C.byref(w), C.byref(p),
+                                          C.byref(k)))
+        return {"panel_rows": r.value, "panel_width": w.value, "panels": p.value,
+                "kernels_per_trial": k.value}
 
     def time_spmv(self, which: str, reps: int = 20) -> float:
         """Mean ms of a plain SpMV with A ("A") or A^T ("At") on the resident iterate."""

@@ -76,6 +76,24 @@ def test_result_is_the_same_alone_and_in_the_mix(batch):
         assert np.array_equal(alone["x"], together[k]["x"])
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_autotuning_leaves_no_trace(batch, precision):
+    """The autotuner times its kernel variants with probe trials on the first
+    work list: they apply no pending average and make no decision.  Every
+    instance's trajectory, hence its iteration count and result, is the same
+    bit for bit with and without tuning."""
+    models = small_mix(seed=12, count=4)
+    tuned = batch.solve_batch(models, matrix_precision=precision, iteration_limit=300000,
+                              time_limit=120, autotune=True)
+    plain = batch.solve_batch(models, matrix_precision=precision, iteration_limit=300000,
+                              time_limit=120, autotune=False)
+    for a, b in zip(tuned, plain):
+        assert a["status"] == b["status"] == "OPTIMAL"
+        assert a["iterations"] == b["iterations"]
+        assert a["objective"] == b["objective"]
+        assert np.array_equal(a["x"], b["x"]) and np.array_equal(a["y"], b["y"])
+
+
 def test_batch_terminal_statuses(batch):
     from tests.test_host import from_rows
     unbounded = presolve_model()

@@ -17,6 +17,12 @@ from tests.test_oracle import halpern_expected, sparse_qp_model, tiny
 pytestmark = pytest.mark.gpu
 
 
+def step_sizes(model):
+    """tau, sigma as solve_continuous starts them (src/solver.cpp:299-333)."""
+    import bench
+    return bench.step_sizes(model)
+
+
 def near(a, b, tol=1e-11):
     a, b = np.asarray(a, dtype=float), np.asarray(b, dtype=float)
     err = np.abs(a - b) / (1 + np.abs(b))
@@ -402,3 +408,69 @@ def test_linear_solve_bicgstab(gpu, fp32):
     assert np.max(np.abs(x - want)) <= tol * (1 + np.max(np.abs(want)))
     if not fp32:
         assert np.linalg.norm(dense @ x - rhs) <= 1e-10 * (1 + np.linalg.norm(rhs)) * 10
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "fp32"])
+def test_panel_path_multi_panel_parity(gpu, oracle, precision):
+    """A's long rows by column panel (the dual SpMV's panel kernel) with more
+    than one panel: 100,000 columns are several panels of the FP64 dx slice a
+    CTA holds (two of the FP32 one).  Fixed steps against the oracle, 1e-10
+    relative in FP64 over 60 trials: a long row is summed per panel in CSR
+    order and the panel sums are added in panel order, where the CPU adds the
+    whole row in CSR order.  With FP32 matrices the oracle gets the same
+    FP32-rounded values (MIXED: FP64 gathers and sums, 1e-10) or the FP32
+    engine is held to 1e-4 (FP32 gathers and sums)."""
+    m = synth.power_law_lp(m=20000, n=100000, nnz=500000, seed=3, len_hi=5000)
+    if precision != "fp64":
+        m.val = m.val.astype(np.float32).astype(np.float64)
+    g = gpu.PdhgBackend(m, graphs=True, precision=precision)
+    info = g.layout_info()
+    assert info["panels"] >= 2 and info["panel_rows"] > 0, info
+    assert info["kernels_per_trial"] == 3
+    cpu = oracle.model(m).backend(np.zeros(m.n), np.zeros(m.m))
+    tol = 1e-4 if precision == "fp32" else 1e-10
+    tau, sigma = step_sizes(m)
+    for _ in range(3):
+        assert cpu.advance(20, tau, sigma) == g.advance(20, tau, sigma)
+        for u, w in zip(g.candidates(), cpu.candidates()):
+            near(u, w, tol)
+
+
+def test_panel_path_single_panel_is_sequential(gpu, oracle):
+    """With every column in one panel a long row's sum is its sequential CSR
+    sum, the CPU's order: fixed-step trajectories agree to 1e-13."""
+    m = synth.power_law_lp(m=3000, n=6000, nnz=60000, seed=4, len_hi=3000)
+    g = gpu.PdhgBackend(m, graphs=True)
+    info = g.layout_info()
+    assert info["panels"] == 1 and info["panel_rows"] > 0, info
+    cpu = oracle.model(m).backend(np.zeros(m.n), np.zeros(m.m))
+    tau, sigma = step_sizes(m)
+    assert cpu.advance(50, tau, sigma) == g.advance(50, tau, sigma)
+    for u, w in zip(g.candidates(), cpu.candidates()):
+        near(u, w, 1e-13)
+
+
+def test_trajectory_parity_above_openmp_threshold(gpu, reference):
+    """Step by step against the reference's own CpuBackend (oracle/_ref, all host
+    threads) above its OpenMP threshold (10,000 rows or columns,
+    src/cpu.cpp:105,123,134), where its step-rule sums are split over threads:
+    a power-law LP of 50,000 x 100,000 with 1,000,000 nonzeros and rows of up to
+    5,000 entries (several column panels on the device).  Adaptive steps,
+    compared at equal accepted counts; tolerance 1e-8 relative after 40
+    accepted steps, as for the oracle runs on smaller power-law LPs: both sides
+    group the sums differently and the adaptive step factor carries the
+    last-bit differences forward."""
+    import os
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    m = synth.power_law_lp(m=50000, n=100000, nnz=1_000_000, seed=6, len_hi=5000)
+    assert int(np.diff(m.ptr).max()) > 4000
+    cpu = reference.model(m).backend(np.zeros(m.n), np.zeros(m.m), adaptive=True)
+    g = gpu.PdhgBackend(m, adaptive=True, graphs=True)
+    assert g.layout_info()["panels"] >= 2
+    tau, sigma = step_sizes(m)
+    done = 0
+    for _ in range(4):
+        done = advance_to(g, done + cpu.advance(10, tau, sigma), tau, sigma, done)
+        assert g.rejected_steps() == cpu.rejected_steps()
+        for u, w in zip(g.candidates(), cpu.candidates()):
+            near(u, w, 1e-8)
