@@ -25,9 +25,6 @@
 #ifndef NK_FUSED_THREADS
 #define NK_FUSED_THREADS 1024 // threads per CTA of the fused trial kernels
 #endif
-#ifndef NK_HOT
-#define NK_HOT 0 // 1: the primal kernel gathers y's leading entries from shared memory
-#endif
 #ifndef NK_SPLIT_PIPE
 #define NK_SPLIT_PIPE 0 // 1: software-pipelined dot for split-row segments
 #endif
@@ -82,7 +79,10 @@ struct Vecs {
     Control *ctl;
     int grid_p;           // CTAs of primal_kernel (partials to read)
     double reflection;
-    int64_t hot;          // leading entries of y each primal CTA copies to shared memory
+    // rows split across chunks: their dx^2 (A^T's rows) and dy^2, dy*delta (A's)
+    double *split_p;      // [At's cross-chunk split rows]
+    double *split_d;      // [2 * A's cross-chunk split rows]
+    int nsplit_p, nsplit_d;
     // panel path of A's long rows (nk_panel.cuh): partial[p * panel_rows + i]
     const double *panel_partial;
     int64_t panel_rows;
@@ -168,19 +168,20 @@ __device__ __forceinline__ bool split_chunk(double *wpart /* this warp's 32 */, 
 // chunk combine.  Kept out of line so that the register budget of the kernels'
 // main path does not carry it.  init_vec (may be null) gives the row sum's
 // start; on true, *row and *total hold the completed row.
-template <class Acc, int G = 0, bool HOT = false, class V, class I, class X>
+// *cross receives the row's counter when the row spans chunks (-1 when it
+// lies in this chunk).
+template <class Acc, int G = 0, class V, class I, class X>
 __device__ __noinline__ bool split_lane(const Sell<V, I> M, int64_t vr, int len,
                                         const X *__restrict__ x, const double *init_vec,
-                                        double *wpart, int64_t *row, double *total,
-                                        const X *hot = nullptr, int64_t nhot = 0) {
+                                        double *wpart, int64_t *row, double *total, int *cross) {
 #if NK_SPLIT_PIPE
     const double part = double(sell_dot_pipelined<Acc, kUnrollSplit>(M, vr, len, Acc(0), x));
 #else
-    const double part =
-        double(sell_dot<Acc, kUnrollSplit, G, HOT>(M, vr, len, Acc(0), x, hot, nhot));
+    const double part = double(sell_dot<Acc, kUnrollSplit, G>(M, vr, len, Acc(0), x));
 #endif
     const int4 sg = M.seg[vr];
     *row = sg.x;
+    *cross = sg.w;
     const double init = (sg.x >= 0 && init_vec) ? init_vec[sg.x] : 0.;
     return split_chunk(wpart, M.slots, M.counters, sg, vr, part, init, total);
 }
@@ -216,24 +217,78 @@ __device__ __forceinline__ int64_t chunk_stride() {
     return (int64_t(gridDim.x) * blockDim.x) >> 5;
 }
 
+// ------------------------------------------------------------------ schedule
+// The fused kernels' schedule: CTA b owns the chunks list[off[b] .. off[b+1])
+// (chosen on the host by memory work, costliest first) and its warps claim
+// them one at a time from a shared counter, so no warp idles while its CTA
+// has work left.  A chunk's contribution to the step rule's sums goes to its
+// own slot (k, its place in the list), and the CTA adds the slots in list
+// order: the sums do not depend on which warp ran which chunk.
+struct CtaClaim {
+    const int64_t *list;
+    int64_t begin;
+    int count;
+    unsigned *counter; // shared, zeroed before the first claim
+    __device__ __forceinline__ bool next(int *k, int64_t *ch) {
+        unsigned c = 0;
+        if ((threadIdx.x & 31) == 0)
+            c = atomicAdd(counter, 1u);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        if (int(c) >= count)
+            return false;
+        *k = int(c);
+        *ch = list[begin + c];
+        return true;
+    }
+};
+
+// Warp sum in a fixed shuffle tree; result in every lane.
+__device__ __forceinline__ double warp_total(double v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+}
+
+// The CTA's NV sums: slots[k*NV + t] of its `count` chunks added in list
+// order by warp 0 (lane-strided, then a fixed tree).  Writes out[t] from
+// thread 0.  Called by every thread after a __syncthreads.
+template <int NV>
+__device__ __forceinline__ void ordered_slots(const double *slots, int count, double *out) {
+    if (threadIdx.x >= 32)
+        return;
+#pragma unroll
+    for (int t = 0; t < NV; ++t) {
+        double s = 0;
+        for (int k = threadIdx.x; k < count; k += 32)
+            s += slots[k * NV + t];
+        s = warp_total(s);
+        if (threadIdx.x == 0)
+            out[t] = s;
+    }
+}
+
 // ------------------------------------------------------------------ primal
 // SPLIT: the matrix has split rows (kernels without them skip that path
-// entirely, which keeps their register footprint small).
-// HOT: the CTA first copies y[0, v.hot) (y32 with FP32 gathers) into dynamic
-// shared memory and gathers those entries from there.  Rows of A are in
-// engine order, longest first, so these are the rows with the most entries,
-// i.e. the y entries that the rows of A^T gather most often.
-template <class Acc, class V, class I, bool SPARSE_Q, bool FP32G, bool SPLIT, bool HOT>
+// entirely, which keeps their register footprint small).  A row split across
+// chunks is finished by whichever warp adds its last segment; its dx^2 goes
+// to that row's own slot (split_p[counter]), added by the decision in row
+// order, so it too lands in the sums the same way every time.
+template <class Acc, class V, class I, bool SPARSE_Q, bool FP32G, bool SPLIT>
 __global__ void __launch_bounds__(kFusedThreads, kFusedMinBlocks)
     primal_kernel(Sell<V, I> At, QCsr<V, I> Q, Vecs v) {
-    __shared__ double red[kFusedWarps];
-    __shared__ double wpart[kFusedWarps][32];
+    __shared__ double wpart[SPLIT ? kFusedWarps : 1][32];
+    __shared__ unsigned claim;
     extern __shared__ __align__(16) unsigned char dyn_smem[];
-    using Y = typename std::conditional<FP32G, float, double>::type;
+    double *slots = reinterpret_cast<double *>(dyn_smem); // one per chunk of this CTA
     const Control &ctl = *v.ctl;
-    double mine = 0;
-    bool bad = false;
-    if (ctl.restart == 0) {
+    const int64_t begin = At.coff[blockIdx.x];
+    const int count = int(At.coff[blockIdx.x + 1] - begin);
+    if (threadIdx.x == 0)
+        claim = 0;
+    __syncthreads();
+    const bool frozen = ctl.restart != 0; // a requested Halpern restart freezes the chunk
+    if (!frozen) {
         const int cur = ctl.cur;
         const bool pending = ctl.pending != 0;
         const double pw = ctl.pending_w;
@@ -242,19 +297,9 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedMinBlocks)
         double *xt = cur ? v.x0 : v.x1;
         const double *y = cur ? v.y1 : v.y0;
         const float *y32 = cur ? v.y32_1 : v.y32_0;
-        Y *hot = reinterpret_cast<Y *>(dyn_smem);
-        if constexpr (HOT) {
-            const Y *ys;
-            if constexpr (FP32G)
-                ys = y32;
-            else
-                ys = y;
-            stage16<kFusedThreads>(hot, ys, v.hot * int64_t(sizeof(Y)));
-            __syncthreads();
-        }
-        // epilogue of column j; g = c_j + (A^T y)_j
+        // epilogue of column j; g = c_j + (A^T y)_j; returns dx_j^2 (inf if not finite)
         auto finish = [&](int64_t j, double g, double xj, double qj, double lj, double uj,
-                          double aj) {
+                          double aj) -> double {
             if (pending)
                 v.xa[j] = aj + (xj - aj) * pw;
             if constexpr (SPARSE_Q)
@@ -267,57 +312,71 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedMinBlocks)
                 v.dx32[j] = float(d);
             else
                 v.dx[j] = d;
-            mine += d * d;
-            bad |= !isfinite(t);
+            return isfinite(t) ? d * d : INFINITY;
         };
         const int lane = threadIdx.x & 31;
-        WarpChunks<V, I> chunks(At);
-        for (int64_t ch; chunks.next(&ch);) {
+        CtaClaim cc{At.clist, begin, count, &claim};
+        int k;
+        for (int64_t ch; cc.next(&k, &ch);) {
             const int64_t vr = ch * 32 + lane;
-            if (vr >= At.nv)
-                continue;
-            const int len = At.len[vr];
-            if (!SPLIT || vr >= At.nsv) {
-                const int64_t j = vr - At.nsv + At.nsr;
+            double mine = 0;
+            if (vr < At.nv) {
+                const int len = At.len[vr];
+                if (!SPLIT || vr >= At.nsv) {
+                    const int64_t j = vr - At.nsv + At.nsr;
 #if NK_PREFETCH // the epilogue's loads do not depend on the dot product: issue them first
-                const double xj = x[j], cj = v.c[j], qj = v.q ? v.q[j] : 0., lj = v.lb[j],
-                             uj = v.ub[j];
-                const double aj = pending ? v.xa[j] : 0.;
+                    const double xj = x[j], cj = v.c[j], qj = v.q ? v.q[j] : 0., lj = v.lb[j],
+                                 uj = v.ub[j];
+                    const double aj = pending ? v.xa[j] : 0.;
 #else
-                const double cj = v.c[j];
+                    const double cj = v.c[j];
 #endif
-                double g;
-                if constexpr (FP32G)
-                    g = cj + double(sell_dot<Acc, kUnroll, 0, HOT>(At, vr, len, Acc(0), y32, hot,
-                                                                   v.hot));
-                else // FP64 accumulation starts from c_j, like the CPU loop (src/cpu.cpp:108-111)
-                    g = double(sell_dot<Acc, kUnroll, 0, HOT>(At, vr, len, Acc(cj), y, hot,
-                                                              v.hot));
-#if NK_PREFETCH
-                finish(j, g, xj, qj, lj, uj, aj);
-#else
-                finish(j, g, x[j], v.q ? v.q[j] : 0., v.lb[j], v.ub[j], pending ? v.xa[j] : 0.);
-#endif
-            } else if constexpr (SPLIT) { // split region: the whole warp is here
-                int64_t j;
-                double g;
-                bool done;
-                if constexpr (FP32G) // FP32 sums add c_j afterwards, in FP64
-                    done = split_lane<Acc, 0, HOT>(At, vr, len, y32, nullptr,
-                                                   wpart[threadIdx.x >> 5], &j, &g, hot, v.hot);
-                else
-                    done = split_lane<Acc, 0, HOT>(At, vr, len, y, v.c, wpart[threadIdx.x >> 5],
-                                                   &j, &g, hot, v.hot);
-                if (done) {
+                    double g;
                     if constexpr (FP32G)
-                        g = v.c[j] + g;
-                    finish(j, g, x[j], v.q ? v.q[j] : 0., v.lb[j], v.ub[j], pending ? v.xa[j] : 0.);
+                        g = cj + double(sell_dot<Acc>(At, vr, len, Acc(0), y32));
+                    else // FP64 accumulation starts from c_j, like the CPU loop (src/cpu.cpp:108-111)
+                        g = double(sell_dot<Acc>(At, vr, len, Acc(cj), y));
+#if NK_PREFETCH
+                    mine = finish(j, g, xj, qj, lj, uj, aj);
+#else
+                    mine = finish(j, g, x[j], v.q ? v.q[j] : 0., v.lb[j], v.ub[j],
+                                  pending ? v.xa[j] : 0.);
+#endif
                 }
             }
+            if constexpr (SPLIT) {
+                if (ch * 32 < At.nsv) { // split region: the whole warp is here
+                    int64_t j;
+                    double g;
+                    int cross = -1;
+                    bool done;
+                    if constexpr (FP32G) // FP32 sums add c_j afterwards, in FP64
+                        done = split_lane<Acc>(At, vr, At.len[vr], y32, nullptr,
+                                               wpart[threadIdx.x >> 5], &j, &g, &cross);
+                    else
+                        done = split_lane<Acc>(At, vr, At.len[vr], y, v.c,
+                                               wpart[threadIdx.x >> 5], &j, &g, &cross);
+                    if (done) {
+                        if constexpr (FP32G)
+                            g = v.c[j] + g;
+                        const double d2 = finish(j, g, x[j], v.q ? v.q[j] : 0., v.lb[j], v.ub[j],
+                                                 pending ? v.xa[j] : 0.);
+                        if (cross >= 0)
+                            v.split_p[cross] = d2;
+                        else
+                            mine = d2;
+                    }
+                }
+            }
+            mine = warp_total(mine);
+            if (lane == 0)
+                slots[k] = mine;
         }
     }
-    double tot[1] = {bad ? INFINITY : mine};
-    cta_sum<1, kFusedWarps>(tot, red);
+    __syncthreads();
+    double tot[1] = {0};
+    if (!frozen)
+        ordered_slots<1>(slots, count, tot);
     if (threadIdx.x == 0)
         v.part_p[blockIdx.x] = tot[0];
 }
@@ -373,19 +432,26 @@ __device__ inline void decide(Vecs &v, double p, double d, double c) {
 }
 
 // PANEL: A's long rows (engine rows [0, v.panel_rows)) come from panel_kernel
-// as one partial sum per column panel; the warp schedule lists them as
-// "combine chunks" (encoded -k-1 for rows [32k, 32k+32)) in place of their
-// split-row chunks, and a lane adds its row's partials in panel order.
+// as one partial sum per column panel; the schedule lists them as "combine
+// chunks" (encoded -k-1 for rows [32k, 32k+32)) in place of their split-row
+// chunks, and a lane adds its row's partials in panel order.
 template <class Acc, class V, class I, bool FP32G, bool SPLIT, bool PANEL = false>
 __global__ void __launch_bounds__(kFusedThreads, kFusedMinBlocks)
     dual_kernel(Sell<V, I> A, Vecs v) {
+    __shared__ double wpart[SPLIT ? kFusedWarps : 1][32];
     __shared__ double red[kFusedWarps * 3];
-    __shared__ double wpart[kFusedWarps][32];
+    __shared__ unsigned claim;
     __shared__ bool last;
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    double *slots = reinterpret_cast<double *>(dyn_smem); // two per chunk of this CTA
     const Control &ctl = *v.ctl;
-    double dy2 = 0, cpl = 0;
-    bool bad = false;
-    if (ctl.restart == 0) {
+    const int64_t begin = A.coff[blockIdx.x];
+    const int count = int(A.coff[blockIdx.x + 1] - begin);
+    if (threadIdx.x == 0)
+        claim = 0;
+    __syncthreads();
+    const bool frozen = ctl.restart != 0;
+    if (!frozen) {
         const int cur = ctl.cur;
         const bool pending = ctl.pending != 0;
         const double pw = ctl.pending_w;
@@ -395,8 +461,9 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedMinBlocks)
         float *yt32 = cur ? v.y32_0 : v.y32_1;
         const double *ax = cur ? v.ax1 : v.ax0;
         double *axt = cur ? v.ax0 : v.ax1;
+        // epilogue of row i; adds dy^2 (inf if not finite) and dy * delta
         auto finish = [&](int64_t i, double delta, double yi, double axi, double rli, double rui,
-                          double ai) {
+                          double ai, double &dy2, double &cpl) {
             if (pending)
                 v.ya[i] = ai + (yi - ai) * pw;
             const double bar = axi + 2 * delta;
@@ -407,74 +474,107 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedMinBlocks)
                 yt32[i] = float(t);
             axt[i] = axi + delta;
             const double dy = t - yi;
-            dy2 += dy * dy;
-            cpl += dy * delta;
-            bad |= !isfinite(bar) || !isfinite(t) || !isfinite(delta);
+            const bool bad = !isfinite(bar) || !isfinite(t) || !isfinite(delta);
+            dy2 = bad ? INFINITY : dy * dy;
+            cpl = dy * delta;
         };
         const int lane = threadIdx.x & 31;
-        WarpChunks<V, I> chunks(A);
-        for (int64_t ch; chunks.next(&ch);) {
+        CtaClaim cc{A.clist, begin, count, &claim};
+        int k;
+        for (int64_t ch; cc.next(&k, &ch);) {
+            double dy2 = 0, cpl = 0;
+            bool combine = false;
             if constexpr (PANEL) {
-                if (ch < 0) { // a long row: its panel partials, in panel order
+                if (ch < 0) { // long rows: their panel partials, in panel order
+                    combine = true;
                     const int64_t i = (-ch - 1) * 32 + lane;
-                    if (i >= v.panel_rows)
-                        continue;
-                    const double yi = y[i], axi = ax[i], rli = v.rl[i], rui = v.ru[i];
-                    const double ai = pending ? v.ya[i] : 0.;
-                    const double *pp = v.panel_partial + i;
-                    const int64_t stride = v.panel_rows;
-                    double delta = 0;
-                    int p = 0;
-                    for (; p + 4 <= v.npanels; p += 4) {
-                        const double a0 = __ldcg(pp + p * stride), a1 = __ldcg(pp + (p + 1) * stride),
-                                     a2 = __ldcg(pp + (p + 2) * stride),
-                                     a3 = __ldcg(pp + (p + 3) * stride);
-                        delta += a0;
-                        delta += a1;
-                        delta += a2;
-                        delta += a3;
+                    if (i < v.panel_rows) {
+                        const double yi = y[i], axi = ax[i], rli = v.rl[i], rui = v.ru[i];
+                        const double ai = pending ? v.ya[i] : 0.;
+                        const double *pp = v.panel_partial + i;
+                        const int64_t stride = v.panel_rows;
+                        double delta = 0;
+                        int p = 0;
+                        constexpr int B = 8; // loads in flight; the adds stay in panel order
+                        for (; p + B <= v.npanels; p += B) {
+                            double a[B];
+#pragma unroll
+                            for (int q = 0; q < B; ++q)
+                                a[q] = __ldcg(pp + (p + q) * stride);
+#pragma unroll
+                            for (int q = 0; q < B; ++q)
+                                delta += a[q];
+                        }
+                        for (; p < v.npanels; ++p)
+                            delta += __ldcg(pp + p * stride);
+                        finish(i, delta, yi, axi, rli, rui, ai, dy2, cpl);
                     }
-                    for (; p < v.npanels; ++p)
-                        delta += __ldcg(pp + p * stride);
-                    finish(i, delta, yi, axi, rli, rui, ai);
-                    continue;
                 }
             }
-            const int64_t vr = ch * 32 + lane;
-            if (vr >= A.nv)
-                continue;
-            const int len = A.len[vr];
-            if (!SPLIT || vr >= A.nsv) {
-                const int64_t i = vr - A.nsv + A.nsr;
+            if (!combine) {
+                const int64_t vr = ch * 32 + lane;
+                if (vr < A.nv && (!SPLIT || vr >= A.nsv)) {
+                    const int len = A.len[vr];
+                    const int64_t i = vr - A.nsv + A.nsr;
 #if NK_PREFETCH
-                const double yi = y[i], axi = ax[i], rli = v.rl[i], rui = v.ru[i];
-                const double ai = pending ? v.ya[i] : 0.;
+                    const double yi = y[i], axi = ax[i], rli = v.rl[i], rui = v.ru[i];
+                    const double ai = pending ? v.ya[i] : 0.;
 #endif
-                double delta;
-                if constexpr (FP32G)
-                    delta = double(sell_dot<Acc, kUnroll, kDualGather>(A, vr, len, Acc(0), v.dx32));
-                else
-                    delta = double(sell_dot<Acc, kUnroll, kDualGather>(A, vr, len, Acc(0), v.dx));
+                    double delta;
+                    if constexpr (FP32G)
+                        delta = double(sell_dot<Acc, kUnroll, kDualGather>(A, vr, len, Acc(0),
+                                                                         v.dx32));
+                    else
+                        delta = double(sell_dot<Acc, kUnroll, kDualGather>(A, vr, len, Acc(0),
+                                                                         v.dx));
 #if NK_PREFETCH
-                finish(i, delta, yi, axi, rli, rui, ai);
+                    finish(i, delta, yi, axi, rli, rui, ai, dy2, cpl);
 #else
-                finish(i, delta, y[i], ax[i], v.rl[i], v.ru[i], pending ? v.ya[i] : 0.);
+                    finish(i, delta, y[i], ax[i], v.rl[i], v.ru[i], pending ? v.ya[i] : 0., dy2,
+                           cpl);
 #endif
-            } else if constexpr (SPLIT) { // split region: the whole warp is here
-                int64_t i;
-                double delta;
-                bool done;
-                if constexpr (FP32G)
-                    done = split_lane<Acc, kDualGather>(A, vr, len, v.dx32, nullptr, wpart[threadIdx.x >> 5], &i, &delta);
-                else
-                    done = split_lane<Acc, kDualGather>(A, vr, len, v.dx, nullptr, wpart[threadIdx.x >> 5], &i, &delta);
-                if (done)
-                    finish(i, delta, y[i], ax[i], v.rl[i], v.ru[i], pending ? v.ya[i] : 0.);
+                }
+                if constexpr (SPLIT) {
+                    if (ch * 32 < A.nsv) { // split region: the whole warp is here
+                        int64_t i;
+                        double delta;
+                        int cross = -1;
+                        bool done;
+                        if constexpr (FP32G)
+                            done = split_lane<Acc, kDualGather>(A, vr, A.len[vr], v.dx32, nullptr,
+                                                                wpart[threadIdx.x >> 5], &i,
+                                                                &delta, &cross);
+                        else
+                            done = split_lane<Acc, kDualGather>(A, vr, A.len[vr], v.dx, nullptr,
+                                                                wpart[threadIdx.x >> 5], &i,
+                                                                &delta, &cross);
+                        if (done) {
+                            double a2, a3;
+                            finish(i, delta, y[i], ax[i], v.rl[i], v.ru[i],
+                                   pending ? v.ya[i] : 0., a2, a3);
+                            if (cross >= 0) {
+                                v.split_d[2 * cross] = a2;
+                                v.split_d[2 * cross + 1] = a3;
+                            } else {
+                                dy2 = a2;
+                                cpl = a3;
+                            }
+                        }
+                    }
+                }
+            }
+            dy2 = warp_total(dy2);
+            cpl = warp_total(cpl);
+            if (lane == 0) {
+                slots[2 * k] = dy2;
+                slots[2 * k + 1] = cpl;
             }
         }
     }
-    double tot[2] = {bad ? INFINITY : dy2, cpl};
-    cta_sum<2, kFusedWarps>(tot, red);
+    __syncthreads();
+    double tot[2] = {0, 0};
+    if (!frozen)
+        ordered_slots<2>(slots, count, tot);
     if (threadIdx.x == 0) {
         v.part_d[2 * blockIdx.x] = tot[0];
         v.part_d[2 * blockIdx.x + 1] = tot[1];
@@ -490,10 +590,16 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedMinBlocks)
     __threadfence();
     double p = 0, d = 0, c = 0;
     for (int b = threadIdx.x; b < v.grid_p; b += kFusedThreads)
-        p += v.part_p[b];
+        p += __ldcg(v.part_p + b);
     for (int b = threadIdx.x; b < int(gridDim.x); b += kFusedThreads) {
-        d += v.part_d[2 * b];
-        c += v.part_d[2 * b + 1];
+        d += __ldcg(v.part_d + 2 * b);
+        c += __ldcg(v.part_d + 2 * b + 1);
+    }
+    for (int r = threadIdx.x; r < v.nsplit_p; r += kFusedThreads)
+        p += __ldcg(v.split_p + r);
+    for (int r = threadIdx.x; r < v.nsplit_d; r += kFusedThreads) {
+        d += __ldcg(v.split_d + 2 * r);
+        c += __ldcg(v.split_d + 2 * r + 1);
     }
     double r3[3] = {p, d, c};
     cta_sum<3, kFusedWarps>(r3, red);

@@ -31,9 +31,6 @@
 #include <thread>
 #include <vector>
 
-#ifndef NK_BALANCED
-#define NK_BALANCED 1 // 1: fused kernels follow the balanced warp schedule, 0: round-robin
-#endif
 #ifndef NK_SPLIT
 #define NK_SPLIT 128 // rows with more entries are split into virtual rows of this length
 #endif
@@ -67,17 +64,17 @@ struct SellMatrix {
     DevBuf<int4> seg;
     DevBuf<double> slots;
     DevBuf<unsigned> counters;
+    int ncounters = 0;              // rows split across chunks
     std::vector<int32_t> chunk_len; // host: padded length of each chunk
-    DevBuf<int64_t> woff, wlist;    // balanced warp schedule of the fused kernels
+    DevBuf<int64_t> coff, clist;    // the fused kernels' per-CTA chunk lists
+    int max_cta_items = 0;          // longest of those lists
 
-    // The view the fused trial kernels use: with the balanced warp schedule
+    // The view the fused trial kernels use: with the per-CTA chunk lists
     // (built for their persistent grid).
     template <class V, class I> Sell<V, I> fused_view() const {
         Sell<V, I> s = view<V, I>();
-#if NK_BALANCED
-        s.woff = woff.p;
-        s.wlist = wlist.p;
-#endif
+        s.coff = coff.p;
+        s.clist = clist.p;
         return s;
     }
 
@@ -103,8 +100,8 @@ struct SellMatrix {
     }
     size_t device_bytes() const {
         return cptr.bytes() + len.bytes() + idx32.bytes() + idx64.bytes() + val64.bytes() +
-               val32.bytes() + seg.bytes() + slots.bytes() + counters.bytes() + woff.bytes() +
-               wlist.bytes();
+               val32.bytes() + seg.bytes() + slots.bytes() + counters.bytes() + coff.bytes() +
+               clist.bytes();
     }
 };
 
@@ -137,35 +134,36 @@ struct QMatrix {
 
 // A's long rows by column panel (nk_panel.cuh), for the dual kernel's A dx.
 struct PanelMatrix {
-    int64_t rows = 0, cols = 0, width = 0, entries = 0, padded = 0;
+    int64_t rows = 0, cols = 0, width = 0, entries = 0, padded = 0, nunits = 0;
     int npanels = 0, vbits = 64, grid = 0;
     size_t smem = 0; // dynamic shared memory of panel_kernel: one dx slice
-    DevBuf<int64_t> uoff, cptr;
-    DevBuf<int4> units;
-    DevBuf<int2> lane;
+    DevBuf<int64_t> cptr, uoff;
+    DevBuf<int4> units; // pieces: {panel, first chunk, end chunk, unit}
     DevBuf<uint16_t> lidx;
     DevBuf<double> val64, partial;
     DevBuf<float> val32;
+    DevBuf<unsigned> claim;
     template <class V> PanelView<V> view() const {
         PanelView<V> P;
         P.rows = rows;
         P.cols = cols;
         P.width = width;
-        P.uoff = uoff.p;
+        P.nunits = nunits;
         P.units = units.p;
+        P.uoff = uoff.p;
         P.cptr = cptr.p;
-        P.lane = lane.p;
         P.lidx = lidx.p;
         if constexpr (sizeof(V) == 8)
             P.val = reinterpret_cast<const V *>(val64.p);
         else
             P.val = reinterpret_cast<const V *>(val32.p);
         P.partial = partial.p;
+        P.claim = claim.p;
         return P;
     }
     size_t device_bytes() const {
-        return uoff.bytes() + cptr.bytes() + units.bytes() + lane.bytes() + lidx.bytes() +
-               val64.bytes() + partial.bytes() + val32.bytes();
+        return cptr.bytes() + uoff.bytes() + units.bytes() + lidx.bytes() + val64.bytes() +
+               partial.bytes() + val32.bytes() + claim.bytes();
     }
 };
 
@@ -272,6 +270,7 @@ void build_sell(SellMatrix &M, int64_t rows, int64_t cols, const std::vector<int
     M.nv = P.nv;
     M.nsv = P.nsv;
     M.nsr = P.nsr;
+    M.ncounters = P.ncounters;
     M.padded = P.cptr.back();
     M.chunk_len.resize(P.cptr.size() - 1);
     for (size_t c = 0; c + 1 < P.cptr.size(); ++c)
@@ -437,23 +436,14 @@ void upload_raw(const nk_csr *H, int vbits, cudaStream_t stream, DevBuf<int64_t>
 }
 
 // The primal kernel instance for a model: sparse Q or not, split rows of A^T
-// or not, staged y entries or not (each leaves unused paths out of the build).
+// or not (each leaves unused paths out of the build).
 template <class V, class I> using PrimalFn = void (*)(Sell<V, I>, QCsr<V, I>, Vecs);
-template <class Acc, class V, class I>
-PrimalFn<V, I> primal_kernel_for(bool sparse_q, bool split, bool hot) {
+template <class Acc, class V, class I> PrimalFn<V, I> primal_kernel_for(bool sparse_q, bool split) {
     constexpr bool F = sizeof(Acc) == 4;
-    if (sparse_q) {
-        if (split)
-            return hot ? primal_kernel<Acc, V, I, true, F, true, true>
-                       : primal_kernel<Acc, V, I, true, F, true, false>;
-        return hot ? primal_kernel<Acc, V, I, true, F, false, true>
-                   : primal_kernel<Acc, V, I, true, F, false, false>;
-    }
-    if (split)
-        return hot ? primal_kernel<Acc, V, I, false, F, true, true>
-                   : primal_kernel<Acc, V, I, false, F, true, false>;
-    return hot ? primal_kernel<Acc, V, I, false, F, false, true>
-               : primal_kernel<Acc, V, I, false, F, false, false>;
+    if (sparse_q)
+        return split ? primal_kernel<Acc, V, I, true, F, true>
+                     : primal_kernel<Acc, V, I, true, F, false>;
+    return split ? primal_kernel<Acc, V, I, false, F, true> : primal_kernel<Acc, V, I, false, F, false>;
 }
 
 // ------------------------------------------------------------------ engine
@@ -476,8 +466,9 @@ struct Engine {
     DevBuf<unsigned> mon_arrive;
     Control *host_ctl = nullptr; // pinned mirror
     int grid_p = 1, grid_d = 1, grid_s = 148;
-    int64_t hot = 0;      // leading y entries the primal kernel stages in shared memory
-    size_t hot_bytes = 0; // its dynamic shared memory per CTA
+    // rows split across chunks: each one's step-rule contributions (A^T: dx^2;
+    // A: dy^2, dy * delta)
+    DevBuf<double> split_p, split_d;
     int64_t accepted = 0, rejected = 0, trials = 0;
     int empty_chunks = 0;
     bool request_restart = false;
@@ -531,7 +522,10 @@ struct Engine {
         v.ctl = ctl.p;
         v.grid_p = grid_p;
         v.reflection = reflection;
-        v.hot = hot;
+        v.split_p = split_p.p;
+        v.split_d = split_d.p;
+        v.nsplit_p = At.ncounters;
+        v.nsplit_d = panels ? 0 : A.ncounters; // with panels A's long rows never split
         v.panel_partial = pan.partial.p;
         v.panel_rows = panels ? pan.rows : 0;
         v.npanels = panels ? pan.npanels : 0;
@@ -547,8 +541,8 @@ struct Engine {
         auto qm = Q.view<V, I>();
         if (ev[0])
             cudaEventRecord(ev[0], stream);
-        primal_kernel_for<Acc, V, I>(sparse_q, At.nsv > 0, hot > 0)<<<grid_p, kFusedThreads,
-                                                                       hot_bytes, stream>>>(at, qm, v);
+        primal_kernel_for<Acc, V, I>(sparse_q, At.nsv > 0)<<<grid_p, kFusedThreads, smem_p(),
+                                                              stream>>>(at, qm, v);
         if (ev[1])
             cudaEventRecord(ev[1], stream);
         if (panels) {
@@ -562,16 +556,22 @@ struct Engine {
                 pan.view<V>(), dxp, ctl.p);
             if (ev[3])
                 cudaEventRecord(ev[3], stream);
-            dual_kernel<Acc, V, I, F32, false, true><<<grid_d, kFusedThreads, 0, stream>>>(a, v);
+            dual_kernel<Acc, V, I, F32, false, true><<<grid_d, kFusedThreads, smem_d(), stream>>>(a,
+                                                                                                v);
         } else if (A.nsv > 0)
-            dual_kernel<Acc, V, I, F32, true><<<grid_d, kFusedThreads, 0, stream>>>(a, v);
+            dual_kernel<Acc, V, I, F32, true><<<grid_d, kFusedThreads, smem_d(), stream>>>(a, v);
         else
-            dual_kernel<Acc, V, I, F32, false><<<grid_d, kFusedThreads, 0, stream>>>(a, v);
+            dual_kernel<Acc, V, I, F32, false><<<grid_d, kFusedThreads, smem_d(), stream>>>(a, v);
         if (ev[2])
             cudaEventRecord(ev[2], stream);
         if (halpern)
             halpern_commit<<<grid_for(std::max(n, m)), kThreads, 0, stream>>>(n, m, v, F32);
     }
+    // dynamic shared memory of the fused kernels: one slot per chunk of a CTA
+    // (the primal kernel's dx^2, the dual kernel's dy^2 and dy * delta)
+    size_t smem_p() const { return size_t(std::max(1, At.max_cta_items)) * sizeof(double); }
+    size_t smem_d() const { return size_t(std::max(1, A.max_cta_items)) * 2 * sizeof(double); }
+
     void launch_trial() {
         if (precision == NK_PRECISION_FP64) {
             if (wide)
@@ -1065,25 +1065,21 @@ struct Engine {
     }
 };
 
-// Balanced warp schedule for a persistent grid of `warps` warps (cta_warps per
-// CTA, all CTAs resident at once: occupancy_grid never launches more).
+// Schedule of the fused kernels over their persistent grid (one CTA per SM of
+// 1024 threads; occupancy_grid never launches more than fit at once).
 //
-// Two costs per chunk of padded length L:
-//  * memory work, what an SM's load/store path spends on it: one scattered
-//    sector per gathered entry, the entries' index and value stream, and the
-//    row epilogue's vector traffic (about 44 L + 70 sectors);
-//  * a warp's chain of dependent round trips: per round of kUnroll entries an
-//    index/value load and then the gathers it feeds, one round per leftover
-//    entry, plus the epilogue (and the segment combine of split rows).
-// Level 1 spreads the chunks over the CTAs by memory work, level 2 over the
-// warps of each CTA by chain length; both are longest-first list scheduling
-// (the next chunk goes to the least-loaded CTA or warp, ties to the lowest
-// index).  Every SM holds the same number of CTAs, so balanced CTAs mean
-// balanced SMs whatever the block scheduler's placement.  Rows are sorted by
-// length, so plain round-robin puts the long split-row chunks on the lowest
-// warps, hence on a subset of the SMs, which then set the kernel's time.
-// Which warp runs a chunk changes no row sum, and the per-CTA partial sums are
-// fixed for a given schedule, so results stay deterministic.
+// The cost of a chunk of padded length L is its memory work, what an SM's load
+// path spends on it: one scattered sector per gathered entry, the entries'
+// index and value stream, and the row epilogue's vector traffic (about
+// 44 L + 70 sectors).  The chunks go to the CTAs by longest-first list
+// scheduling on that cost (the next chunk to the least-loaded CTA, ties to the
+// lowest index); inside a CTA the warps claim them dynamically, costliest
+// first, so a slow chunk does not leave the rest of its CTA idle.  Every SM
+// holds the same number of CTAs, so balanced CTAs mean balanced SMs whatever
+// the block scheduler's placement.  Rows are sorted by length, so plain
+// round-robin would put the long split-row chunks on the lowest CTAs.  Which
+// warp or CTA runs a chunk changes no row sum, and the step rule's sums are
+// added in list order, so results stay deterministic.
 
 // Longest-first list scheduling: items (by index into cost) go, costliest
 // first, to the least-loaded machine (ties to the lowest index); owner[k] is
@@ -1106,107 +1102,78 @@ std::vector<int64_t> lpt_assign(const std::vector<int64_t> &items, const std::ve
     return order;
 }
 
-// The two-level schedule of `ids` (item k is ids[k], with memory work work[k]
-// and chain length chain[k]) onto `warps` persistent warps in CTAs of
-// cta_warps; uploads each warp's list (woff, wlist).
-void schedule_items(const std::vector<int64_t> &ids, const std::vector<int64_t> &work,
-                    const std::vector<int64_t> &chain, int64_t warps, int cta_warps,
-                    DevBuf<int64_t> &woff, DevBuf<int64_t> &wlist, cudaStream_t s) {
+// The schedule of `ids` (item k is ids[k], with memory work work[k]) onto
+// `ctas` persistent CTAs: longest-first list scheduling by memory work, then
+// each CTA's items costliest first (its warps claim them in that order).
+// Uploads the per-CTA lists (off, list); returns the longest list.
+int schedule_items(const std::vector<int64_t> &ids, const std::vector<int64_t> &work,
+                   int64_t ctas, DevBuf<int64_t> &off_d, DevBuf<int64_t> &list_d,
+                   cudaStream_t s) {
     const int64_t nit = int64_t(ids.size());
-    const int64_t ctas = std::max<int64_t>(1, warps / cta_warps);
-    warps = ctas * cta_warps;
+    ctas = std::max<int64_t>(1, ctas);
     std::vector<int64_t> all(static_cast<size_t>(nit)), cta(static_cast<size_t>(nit));
     for (int64_t k = 0; k < nit; ++k)
         all[size_t(k)] = k;
-    lpt_assign(all, work, ctas, cta);
-    // items of each CTA, then its warps
-    std::vector<int64_t> cstart(static_cast<size_t>(ctas + 1), 0);
+    const std::vector<int64_t> order = lpt_assign(all, work, ctas, cta); // costliest first
+    std::vector<int64_t> off(static_cast<size_t>(ctas + 1), 0);
     for (int64_t k = 0; k < nit; ++k)
-        ++cstart[size_t(cta[size_t(k)] + 1)];
-    for (int64_t b = 0; b < ctas; ++b)
-        cstart[size_t(b + 1)] += cstart[size_t(b)];
-    std::vector<int64_t> byitem(static_cast<size_t>(std::max<int64_t>(1, nit)));
-    {
-        std::vector<int64_t> pos(cstart.begin(), cstart.end() - 1);
-        for (int64_t k = 0; k < nit; ++k)
-            byitem[size_t(pos[size_t(cta[size_t(k)])]++)] = k;
-    }
-    std::vector<int64_t> off(static_cast<size_t>(warps + 1), 0), seq;
-    seq.reserve(size_t(nit));
-    std::vector<int64_t> local_owner(static_cast<size_t>(nit));
-    std::vector<std::vector<int64_t>> lists(static_cast<size_t>(cta_warps));
+        ++off[size_t(cta[size_t(k)] + 1)];
+    int longest = 0;
     for (int64_t b = 0; b < ctas; ++b) {
-        std::vector<int64_t> mine(byitem.begin() + cstart[size_t(b)],
-                                  byitem.begin() + cstart[size_t(b + 1)]);
-        for (auto &l : lists)
-            l.clear();
-        for (int64_t k : lpt_assign(mine, chain, cta_warps, local_owner))
-            lists[size_t(local_owner[size_t(k)])].push_back(k);
-        for (int w = 0; w < cta_warps; ++w) {
-            off[size_t(b * cta_warps + w + 1)] = int64_t(lists[size_t(w)].size());
-            for (int64_t k : lists[size_t(w)])
-                seq.push_back(ids[size_t(k)]);
-        }
+        longest = std::max(longest, int(off[size_t(b + 1)]));
+        off[size_t(b + 1)] += off[size_t(b)];
     }
-    for (int64_t w = 0; w < warps; ++w)
-        off[size_t(w + 1)] += off[size_t(w)];
-    if (int64_t(seq.size()) != nit || off[size_t(warps)] != nit)
-        throw Error(NK_ERR_INVALID, "internal: warp schedule size");
+    std::vector<int64_t> list(static_cast<size_t>(std::max<int64_t>(1, nit)), 0);
+    {
+        std::vector<int64_t> pos(off.begin(), off.end() - 1);
+        for (int64_t k : order)
+            list[size_t(pos[size_t(cta[size_t(k)])]++)] = ids[size_t(k)];
+    }
     {   // every item exactly once
-        std::vector<int64_t> got(seq), want(ids);
+        std::vector<int64_t> got(list.begin(), list.begin() + nit), want(ids);
         std::sort(got.begin(), got.end());
         std::sort(want.begin(), want.end());
         if (got != want)
-            throw Error(NK_ERR_INVALID, "internal: warp schedule is not a permutation");
+            throw Error(NK_ERR_INVALID, "internal: chunk schedule is not a permutation");
     }
-    if (seq.empty())
-        seq.push_back(0);
-    upload_vector(woff, off, s);
-    upload_vector(wlist, seq, s);
+    upload_vector(off_d, off, s);
+    upload_vector(list_d, list, s);
+    return longest;
 }
 
-// Memory work and chain length of a SELL chunk of padded length L (see above).
-void chunk_costs(int64_t L, bool split, int64_t *work, int64_t *chain) {
-    const int64_t u = split ? kUnrollSplit : kUnroll;
-    *work = 44 * L + (split ? 100 : 70);
-    *chain = (split && NK_SPLIT_PIPE ? (L + u - 1) / u + 1 : 2 * (L / u) + 2 * (L % u)) +
-             (split ? 6 : 4);
-}
+// Memory work of a SELL chunk of padded length L (see above).
+int64_t chunk_work(int64_t L, bool split) { return 44 * L + (split ? 100 : 70); }
 
-void build_schedule(SellMatrix &M, int64_t warps, int cta_warps, cudaStream_t s) {
+void build_schedule(SellMatrix &M, int64_t ctas, cudaStream_t s) {
     const int64_t nch = int64_t(M.chunk_len.size());
     const int64_t split_chunks = M.nsv / 32;
-    std::vector<int64_t> ids(static_cast<size_t>(nch)), work(ids.size()), chain(ids.size());
+    std::vector<int64_t> ids(static_cast<size_t>(nch)), work(ids.size());
     for (int64_t c = 0; c < nch; ++c) {
         ids[size_t(c)] = c;
-        chunk_costs(M.chunk_len[size_t(c)], c < split_chunks, &work[size_t(c)], &chain[size_t(c)]);
+        work[size_t(c)] = chunk_work(M.chunk_len[size_t(c)], c < split_chunks);
     }
-    schedule_items(ids, work, chain, warps, cta_warps, M.woff, M.wlist, s);
+    M.max_cta_items = schedule_items(ids, work, ctas, M.coff, M.clist, s);
 }
 
 // The dual kernel's schedule when A's long rows take the panel path: the
 // chunks past the split region, plus one combine chunk per 32 long rows
 // (encoded -k-1), whose lanes each read `npanels` partials (8 sectors per
 // panel for the warp) and run the row epilogue.
-void build_dual_panel_schedule(SellMatrix &M, int64_t long_rows, int npanels, int64_t warps,
-                               int cta_warps, cudaStream_t s) {
+void build_dual_panel_schedule(SellMatrix &M, int64_t long_rows, int npanels, int64_t ctas,
+                               cudaStream_t s) {
     const int64_t nch = int64_t(M.chunk_len.size());
     const int64_t split_chunks = M.nsv / 32;
     const int64_t combine = (long_rows + 31) / 32;
-    std::vector<int64_t> ids, work, chain;
+    std::vector<int64_t> ids, work;
     for (int64_t k = 0; k < combine; ++k) {
         ids.push_back(-k - 1);
         work.push_back(8 * int64_t(npanels) + 70);
-        chain.push_back(npanels / 4 + 4);
     }
     for (int64_t c = split_chunks; c < nch; ++c) {
-        int64_t w = 0, ch = 0;
-        chunk_costs(M.chunk_len[size_t(c)], false, &w, &ch);
         ids.push_back(c);
-        work.push_back(w);
-        chain.push_back(ch);
+        work.push_back(chunk_work(M.chunk_len[size_t(c)], false));
     }
-    schedule_items(ids, work, chain, warps, cta_warps, M.woff, M.wlist, s);
+    M.max_cta_items = schedule_items(ids, work, ctas, M.coff, M.clist, s);
 }
 
 // Persistent grid: as many CTAs as fit on the device at once, at most one warp
@@ -1241,13 +1208,6 @@ size_t smem_budget(const void *kernel, int ctas_per_sm) {
     b = std::min<int64_t>(b, int64_t(optin) - int64_t(fa.sharedSizeBytes));
     return size_t(std::max<int64_t>(0, b) & ~int64_t(15));
 }
-size_t hot_budget(const void *kernel) {
-    size_t b = smem_budget(kernel, kFusedMinBlocks);
-#ifdef NK_HOT_MAX_BYTES
-    b = std::min<size_t>(b, size_t(NK_HOT_MAX_BYTES));
-#endif
-    return b;
-}
 
 // The panel kernel instance of a precision, with its dynamic shared memory
 // raised to `bytes`; returns the kernel and the budget it allows.
@@ -1261,8 +1221,8 @@ const void *panel_kernel_for(int precision) {
 
 // Panel layout (nk_panel.cuh) of the first `rows` rows of an engine-order CSR
 // (host ptr; device int64 indices and double values), panels of `width`
-// columns, work units spread over `grid` CTAs.  Built on the host from one
-// download of those rows' entries.
+// columns, work units sized for `grid` CTAs to claim.  Built on the host from
+// one download of those rows' entries.
 void build_panels(PanelMatrix &P, int64_t rows, int64_t cols, const std::vector<int64_t> &ptr,
                   const int64_t *didx, const double *dval, int64_t width, int vbits, int grid,
                   size_t xsize, cudaStream_t s) {
@@ -1284,108 +1244,139 @@ void build_panels(PanelMatrix &P, int64_t rows, int64_t cols, const std::vector<
                    "panel value download");
         cuda_check(cudaStreamSynchronize(s), "panel download");
     }
-    // entries of each (panel, row)
-    std::vector<int32_t> cnt(size_t(np * rows), 0);
+    // entries of each (panel, row): a segment of cnt entries plus its marker
+    std::vector<int64_t> cnt(size_t(np * rows), 0);
     for (int64_t r = 0; r < rows; ++r)
         for (int64_t k = ptr[size_t(r)]; k < ptr[size_t(r + 1)]; ++k)
             ++cnt[size_t((hidx[size_t(k)] / width) * rows + r)];
-    // per panel: its rows with entries, most entries first (stable), in chunks of 32
-    std::vector<int32_t> rank(size_t(np * rows), -1);
-    std::vector<int64_t> first_chunk(size_t(np + 1), 0), cptr(1, 0);
-    std::vector<int2> lanes;
-    std::vector<int64_t> chunk_panel;
-    std::vector<int64_t> list;
+    // units: one per CTA, each an equal share of all panels' entries (marker
+    // entries included).  A unit holds one piece per panel it touches; a piece
+    // is one chunk per warp, and the piece's segments go onto its
+    // kPanelThreads lanes longest first onto the least-loaded lane, so every
+    // lane of a unit carries nearly the same stream length.  A panel's
+    // segments (most entries first) go to its pieces by remaining quota.  A
+    // segment's place is (lane, first step) in its piece, then its first
+    // entry's offset.
+    int64_t grand = 0;
+    for (int64_t v : cnt)
+        grand += v > 0 ? v + 1 : 0;
+    const int64_t nunits_target = std::max<int64_t>(1, std::min<int64_t>(
+        grid, (grand + kPanelThreads - 1) / kPanelThreads)); // at least a segment per lane
+    const double share = double(grand) / double(nunits_target);
+    std::vector<int64_t> place(size_t(np * rows), -1);
+    std::vector<int64_t> cptr(1, 0);
+    std::vector<int4> pieces;          // {panel, first chunk, end chunk, unit}
+    std::vector<int64_t> segs, load, quota_left;
+    using Slot = std::pair<int64_t, int64_t>; // (load, lane)
+    double filled = 0;                 // entries placed in units before this panel
     for (int64_t p = 0; p < np; ++p) {
-        const int32_t *cp = cnt.data() + p * rows;
-        list.clear();
+        const int64_t *cp = cnt.data() + p * rows;
+        segs.clear();
+        int64_t total = 0;
         for (int64_t r = 0; r < rows; ++r)
-            if (cp[r] > 0)
-                list.push_back(r);
-        std::stable_sort(list.begin(), list.end(),
-                         [&](int64_t a, int64_t b) { return cp[a] > cp[b]; });
-        for (size_t q = 0; q < list.size(); ++q)
-            rank[size_t(p * rows + list[q])] = int32_t(q);
-        const int64_t nch = (int64_t(list.size()) + 31) / 32;
-        for (int64_t c = 0; c < nch; ++c) {
-            int32_t top = 0;
-            for (int t = 0; t < 32; ++t) {
-                const size_t q = size_t(c * 32 + t);
-                if (q < list.size()) {
-                    lanes.push_back(make_int2(int(list[q]), cp[list[q]]));
-                    top = std::max(top, cp[list[q]]);
-                } else
-                    lanes.push_back(make_int2(-1, 0));
+            if (cp[r] > 0) {
+                segs.push_back(r);
+                total += cp[r] + 1;
             }
-            cptr.push_back(cptr.back() + 32 * int64_t(top));
-            chunk_panel.push_back(p);
+        if (segs.empty())
+            continue;
+        std::stable_sort(segs.begin(), segs.end(),
+                         [&](int64_t a, int64_t b) { return cp[a] > cp[b]; });
+        // the units this panel's entries fall in, and each one's quota
+        const int64_t u0 = std::min<int64_t>(nunits_target - 1, int64_t(filled / share));
+        const int64_t u1 = std::min<int64_t>(nunits_target - 1,
+                                             int64_t((filled + total - 1e-9) / share));
+        quota_left.assign(size_t(u1 - u0 + 1), 0);
+        for (int64_t u = u0; u <= u1; ++u) {
+            const double lo = std::max(filled, double(u) * share);
+            const double hi = u == nunits_target - 1 ? filled + total
+                                                     : std::min(filled + total, (u + 1) * share);
+            quota_left[size_t(u - u0)] = std::max<int64_t>(0, int64_t(hi - lo + 0.5));
         }
-        first_chunk[size_t(p + 1)] = first_chunk[size_t(p)] + nch;
+        filled += total;
+        std::vector<std::vector<int64_t>> piece_segs(quota_left.size());
+        for (int64_t r : segs) {
+            size_t best = 0;
+            for (size_t q = 1; q < quota_left.size(); ++q)
+                if (quota_left[q] > quota_left[best])
+                    best = q;
+            piece_segs[best].push_back(r);
+            quota_left[best] -= cp[r] + 1;
+        }
+        for (size_t q = 0; q < piece_segs.size(); ++q) {
+            if (piece_segs[q].empty())
+                continue;
+            const int64_t c0 = int64_t(cptr.size()) - 1;
+            load.assign(size_t(kPanelThreads), 0);
+            std::priority_queue<Slot, std::vector<Slot>, std::greater<Slot>> heap;
+            for (int64_t l = 0; l < kPanelThreads; ++l)
+                heap.push({0, l});
+            for (int64_t r : piece_segs[q]) {
+                Slot t = heap.top();
+                heap.pop();
+                place[size_t(p * rows + r)] = t.second * (int64_t(1) << 20) + t.first;
+                heap.push({t.first + cp[r] + 1, t.second});
+                load[size_t(t.second)] = t.first + cp[r] + 1;
+            }
+            for (int64_t c = 0; c < kPanelWarps; ++c) {
+                int64_t top = 0;
+                for (int t = 0; t < 32; ++t)
+                    top = std::max(top, load[size_t(c * 32 + t)]);
+                cptr.push_back(cptr.back() + 32 * top);
+            }
+            for (int64_t r : piece_segs[q]) { // (lane, step) -> offset of the first entry
+                const int64_t lane = place[size_t(p * rows + r)] >> 20,
+                              step = place[size_t(p * rows + r)] & ((int64_t(1) << 20) - 1);
+                place[size_t(p * rows + r)] = cptr[size_t(c0 + lane / 32)] + 32 * step + lane % 32;
+            }
+            pieces.push_back(make_int4(int(p), int(c0), int(c0 + kPanelWarps), int(u0 + q)));
+        }
     }
-    const int64_t nchunks = first_chunk[size_t(np)];
     P.padded = cptr.back();
     std::vector<uint16_t> hl(static_cast<size_t>(std::max<int64_t>(1, P.padded)), 0);
     std::vector<double> hv64(vbits == 64 ? size_t(std::max<int64_t>(1, P.padded)) : 1, 0.);
     std::vector<float> hv32(vbits == 64 ? 1 : size_t(std::max<int64_t>(1, P.padded)), 0.f);
-    std::vector<int32_t> &fill = cnt; // reused: entries placed so far per (panel, row)
-    std::fill(fill.begin(), fill.end(), 0);
-    for (int64_t r = 0; r < rows; ++r)
+    auto put = [&](int64_t at, uint16_t j, double v, int64_t row) {
+        hl[size_t(at)] = j;
+        if (j == kPanelMarker) {
+            if (vbits == 64)
+                std::memcpy(&hv64[size_t(at)], &row, 8);
+            else {
+                const int32_t r32 = int32_t(row);
+                std::memcpy(&hv32[size_t(at)], &r32, 4);
+            }
+        } else if (vbits == 64)
+            hv64[size_t(at)] = v;
+        else
+            hv32[size_t(at)] = float(v);
+    };
+    for (int64_t r = 0; r < rows; ++r) {
         for (int64_t k = ptr[size_t(r)]; k < ptr[size_t(r + 1)]; ++k) {
             const int64_t j = hidx[size_t(k)], p = j / width;
-            const int64_t q = rank[size_t(p * rows + r)];
-            const int64_t c = first_chunk[size_t(p)] + q / 32;
-            const int64_t at = cptr[size_t(c)] + 32 * int64_t(fill[size_t(p * rows + r)]++) + q % 32;
-            hl[size_t(at)] = uint16_t(j - p * width);
-            if (vbits == 64)
-                hv64[size_t(at)] = hval[size_t(k)];
-            else
-                hv32[size_t(at)] = float(hval[size_t(k)]);
+            int64_t &at = place[size_t(p * rows + r)];
+            put(at, uint16_t(j - p * width), hval[size_t(k)], 0);
+            at += 32; // the lane's next step
         }
-    // work units: runs of one panel's chunks, about two per CTA; cost in bytes
-    // (index and value stream, lane records, partial writes) plus half the
-    // slice copy, which comes from L2
-    const int64_t vsize = vbits / 8;
-    std::vector<int64_t> ccost(static_cast<size_t>(nchunks));
-    int64_t total = 0;
-    for (int64_t c = 0; c < nchunks; ++c) {
-        ccost[size_t(c)] = (cptr[size_t(c + 1)] - cptr[size_t(c)]) * (2 + vsize) + 32 * 16;
-        total += ccost[size_t(c)];
+        for (int64_t p = 0; p < np; ++p)
+            if (cnt[size_t(p * rows + r)] > 0)
+                put(place[size_t(p * rows + r)], kPanelMarker, 0., r);
     }
-    const int64_t target = std::max<int64_t>(1, total / std::max<int64_t>(1, 2 * int64_t(grid)));
-    std::vector<int4> units;
-    std::vector<int64_t> ucost;
-    for (int64_t p = 0; p < np; ++p) {
-        const int64_t cols_p = std::min(width, cols - p * width);
-        int64_t c = first_chunk[size_t(p)];
-        while (c < first_chunk[size_t(p + 1)]) {
-            int64_t e = c, w = 0;
-            while (e < first_chunk[size_t(p + 1)] && (e == c || w + ccost[size_t(e)] <= target))
-                w += ccost[size_t(e++)];
-            units.push_back(make_int4(int(p), int(c), int(e), 0));
-            ucost.push_back(w + cols_p * int64_t(xsize) / 2);
-            c = e;
-        }
-    }
-    const int64_t nunits = int64_t(units.size());
-    std::vector<int64_t> ids(static_cast<size_t>(nunits)), owner(static_cast<size_t>(nunits));
-    std::iota(ids.begin(), ids.end(), 0);
-    lpt_assign(ids, ucost, grid, owner);
-    std::vector<int64_t> uoff(size_t(grid + 1), 0);
-    for (int64_t u = 0; u < nunits; ++u)
-        ++uoff[size_t(owner[size_t(u)] + 1)];
-    for (int b = 0; b < grid; ++b)
-        uoff[size_t(b + 1)] += uoff[size_t(b)];
-    std::vector<int4> ordered(static_cast<size_t>(std::max<int64_t>(1, nunits)));
-    {
-        std::vector<int64_t> pos(uoff.begin(), uoff.end() - 1);
-        for (int64_t u = 0; u < nunits; ++u)
-            ordered[size_t(pos[size_t(owner[size_t(u)])]++)] = units[size_t(u)];
-    }
+    // pieces in unit order; unit u runs pieces [uoff[u], uoff[u+1])
+    std::stable_sort(pieces.begin(), pieces.end(),
+                     [](const int4 &a, const int4 &b) { return a.w < b.w; });
+    std::vector<int64_t> uoff(size_t(nunits_target + 1), 0);
+    for (const int4 &pc : pieces)
+        ++uoff[size_t(pc.w + 1)];
+    for (int64_t u = 0; u < nunits_target; ++u)
+        uoff[size_t(u + 1)] += uoff[size_t(u)];
+    P.nunits = nunits_target;
+    if (pieces.empty())
+        pieces.push_back(make_int4(0, 0, 0, 0));
+    upload_vector(P.units, pieces, s);
     upload_vector(P.uoff, uoff, s);
-    upload_vector(P.units, ordered, s);
+    P.claim.alloc(2);
+    cuda_check(cudaMemsetAsync(P.claim.p, 0, P.claim.bytes(), s), "panel claims");
     upload_vector(P.cptr, cptr, s);
-    if (lanes.empty())
-        lanes.push_back(make_int2(-1, 0));
-    upload_vector(P.lane, lanes, s);
     upload_vector(P.lidx, hl, s);
     if (vbits == 64)
         upload_vector(P.val64, hv64, s);
@@ -1396,30 +1387,41 @@ void build_panels(PanelMatrix &P, int64_t rows, int64_t cols, const std::vector<
     cuda_check(cudaStreamSynchronize(s), "panel build");
 }
 
+// Kernel instances and persistent grids of an engine.  The fused kernels'
+// grids hold exactly the CTAs that fit on the device at once; their slot
+// memory is sized after the schedules are built (attach_slots).
 template <class Acc, class V, class I> void configure(Engine &E) {
     constexpr bool F32 = sizeof(Acc) == 4;
-    const bool ds = E.A.nsv > 0;
-    E.hot = 0;
-    E.hot_bytes = 0;
-    if (NK_HOT && E.m > 0) {
-        const void *pk = (const void *)primal_kernel_for<Acc, V, I>(E.sparse_q, E.At.nsv > 0, true);
-        const size_t ysize = F32 ? sizeof(float) : sizeof(double);
-        E.hot = std::min<int64_t>(E.m, int64_t(hot_budget(pk) / ysize));
-        E.hot_bytes = size_t((E.hot * int64_t(ysize) + 15) & ~int64_t(15));
-        if (E.hot > 0)
-            cuda_check(cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            int(E.hot_bytes)),
-                       "primal shared memory");
-        else
-            E.hot_bytes = 0;
-    }
-    const void *pk = (const void *)primal_kernel_for<Acc, V, I>(E.sparse_q, E.At.nsv > 0, E.hot > 0);
-    const void *dk = E.panels ? (const void *)dual_kernel<Acc, V, I, F32, false, true>
-                     : ds     ? (const void *)dual_kernel<Acc, V, I, F32, true>
-                              : (const void *)dual_kernel<Acc, V, I, F32, false>;
-    E.grid_p = occupancy_grid(pk, (E.At.nv + 31) / 32, kFusedThreads, E.hot_bytes);
+    const void *pk = (const void *)primal_kernel_for<Acc, V, I>(E.sparse_q, E.At.nsv > 0);
+    const void *dk = E.panels           ? (const void *)dual_kernel<Acc, V, I, F32, false, true>
+                     : E.A.nsv > 0 ? (const void *)dual_kernel<Acc, V, I, F32, true>
+                                        : (const void *)dual_kernel<Acc, V, I, F32, false>;
+    // the slot arrays stay far below the default 48 KB; the grids are sized
+    // without them, which the occupancy check after the schedules confirms
+    E.grid_p = occupancy_grid(pk, (E.At.nv + 31) / 32, kFusedThreads, 0);
     E.grid_d = occupancy_grid(dk, (E.A.nv + 31) / 32, kFusedThreads, 0);
     E.grid_s = occupancy_grid((const void *)spmv_kernel<V, I>, int64_t(1) << 40);
+}
+template <class Acc, class V, class I> void attach_slots(Engine &E) {
+    constexpr bool F32 = sizeof(Acc) == 4;
+    const void *pk = (const void *)primal_kernel_for<Acc, V, I>(E.sparse_q, E.At.nsv > 0);
+    const void *dk = E.panels           ? (const void *)dual_kernel<Acc, V, I, F32, false, true>
+                     : E.A.nsv > 0 ? (const void *)dual_kernel<Acc, V, I, F32, true>
+                                        : (const void *)dual_kernel<Acc, V, I, F32, false>;
+    for (auto [k, bytes, grid] : {std::tuple<const void *, size_t, int>{pk, E.smem_p(), E.grid_p},
+                                  {dk, E.smem_d(), E.grid_d}}) {
+        if (bytes > 48 * 1024)
+            cuda_check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            int(bytes)),
+                       "slot memory");
+        int per = 0, dev = 0, sms = 148;
+        cuda_check(cudaGetDevice(&dev), "device");
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, kFusedThreads, bytes),
+                   "occupancy");
+        if (int64_t(per) * sms < grid)
+            throw Error(NK_ERR_UNSUPPORTED, "fused kernel grid does not fit the device");
+    }
 }
 
 Engine *create_engine(const nk_csr *Ah, const nk_csr *Qh, const double *hc, const double *hq,
@@ -1506,15 +1508,24 @@ Engine *create_engine(const nk_csr *Ah, const nk_csr *Qh, const double *hc, cons
         build_sell(E->A, m, n, pptr, pi.p, pv.p, E->wide, vbits, s);
         // A's long rows (the SELL's split rows) also by column panel, for the dual
         // kernel: panels as wide as one CTA's shared memory holds dx entries, at
-        // most 65536 columns (16-bit offsets), a multiple of 16
-        if (NK_PANEL && NK_BALANCED && E->A.nsr > 0 && n > 0) { // the combine chunks
-                                                                 // live in the schedule
+        // most 65535 columns (16-bit offsets, one value kept for markers), a
+        // multiple of 16
+        if (NK_PANEL && E->A.nsr > 0 && n > 0) {
             const void *pk = panel_kernel_for(o->precision);
             const int64_t xsize = o->precision == NK_PRECISION_FP32 ? 4 : 8;
-            int64_t width = std::min<int64_t>(65536, int64_t(smem_budget(pk, kPanelMinBlocks)) / xsize);
+            int64_t width = std::min<int64_t>(kPanelMaxWidth,
+                                              int64_t(smem_budget(pk, kPanelMinBlocks)) / xsize);
             width = std::min<int64_t>(width, (n + 15) / 16 * 16) / 16 * 16;
             const int64_t np = width > 0 ? (n + width - 1) / width : 0;
-            if (width >= 16 && np * E->A.nsr <= (int64_t(1) << 25)) {
+            // worth it only where the long rows' entries come in long runs per
+            // panel: the stream then runs at memory speed, while a panel's
+            // segments of a few entries each cost about what their gathers do
+            int64_t long_entries = 0;
+            for (int64_t i = 0; i < E->A.nsr; ++i)
+                long_entries += pptr[size_t(i + 1)] - pptr[size_t(i)];
+            const bool long_runs =
+                width >= 16 && long_entries >= NK_PANEL_MIN_RUN * np * E->A.nsr;
+            if (long_runs && np * E->A.nsr <= (int64_t(1) << 25)) {
                 const size_t smem = size_t(width * xsize);
                 cuda_check(cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 int(smem)),
@@ -1652,12 +1663,21 @@ Engine *create_engine(const nk_csr *Ah, const nk_csr *Qh, const double *hc, cons
         E->wide ? configure<double, float, int64_t>(*E) : configure<double, float, int32_t>(*E);
     else
         E->wide ? configure<float, float, int64_t>(*E) : configure<float, float, int32_t>(*E);
-    build_schedule(E->At, int64_t(E->grid_p) * kFusedWarps, kFusedWarps, s);
+    build_schedule(E->At, E->grid_p, s);
     if (E->panels)
-        build_dual_panel_schedule(E->A, E->pan.rows, E->pan.npanels,
-                                  int64_t(E->grid_d) * kFusedWarps, kFusedWarps, s);
+        build_dual_panel_schedule(E->A, E->pan.rows, E->pan.npanels, E->grid_d, s);
     else
-        build_schedule(E->A, int64_t(E->grid_d) * kFusedWarps, kFusedWarps, s);
+        build_schedule(E->A, E->grid_d, s);
+    if (o->precision == NK_PRECISION_FP64)
+        E->wide ? attach_slots<double, double, int64_t>(*E) : attach_slots<double, double, int32_t>(*E);
+    else if (o->precision == NK_PRECISION_MIXED)
+        E->wide ? attach_slots<double, float, int64_t>(*E) : attach_slots<double, float, int32_t>(*E);
+    else
+        E->wide ? attach_slots<float, float, int64_t>(*E) : attach_slots<float, float, int32_t>(*E);
+    E->split_p.alloc(size_t(std::max(1, E->At.ncounters)));
+    E->split_d.alloc(size_t(2 * std::max(1, E->A.ncounters)));
+    cuda_check(cudaMemsetAsync(E->split_p.p, 0, E->split_p.bytes(), s), "split slots");
+    cuda_check(cudaMemsetAsync(E->split_d.p, 0, E->split_d.bytes(), s), "split slots");
     E->part_p.alloc(size_t(E->grid_p));
     E->part_d.alloc(size_t(2 * E->grid_d));
     E->ctl.alloc(1);

@@ -11,15 +11,27 @@
 // slice once and reads every gathered dx entry of the panel from shared memory
 // (a few bank cycles per warp instead of one lookup per lane).
 //
-// Inside a panel the rows with at least one entry there are ordered by their
-// entry count (descending, stable) and cut into 32-row chunks stored
-// column-major, one row per lane, as in SELL-32: entry k of the chunk's lane t
-// sits at cptr[c] + 32*k + t, and a row's entries keep their CSR order.  A lane
-// adds its row's entries in the panel one by one from zero and writes the sum
-// to partial[p*rows + row]; (row, panel) pairs without entries are never
-// written and stay zero.  The dual kernel then adds a long row's partials in
-// panel order 0, 1, ..., from zero: the result does not depend on timing, and
-// with a single panel it is the row's sequential CSR sum, the CPU's order.
+// Inside a panel each row with entries there is a segment: its entries in CSR
+// order followed by a marker entry (column 0xFFFF) whose value slot carries
+// the row's index.  Segments are packed whole into lanes, longest first onto
+// the least-loaded lane, so every lane holds a stream of nearly the same
+// length.
+// A chunk's 32 lane streams are stored column-major as in SELL-32 (entry k of
+// lane t of chunk c at cptr[c] + 32*k + t).  A lane adds its entries one by one; at a marker
+// it writes the sum to partial[p*rows + row] and starts again from zero.  So a
+// row's panel sum is its sequential CSR sum over that panel, and no lane waits
+// on a lookup: the row number arrives in the stream.  (row, panel) pairs
+// without entries are never written and stay zero.  The dual kernel then adds
+// a long row's partials in panel order 0, 1, ..., from zero: the result does
+// not depend on timing, and with a single panel it is the row's sequential CSR
+// sum, the CPU's order.
+//
+// A unit is an equal share of all panels' entries, one per CTA; it holds one
+// piece (one chunk per warp) per panel it touches, so a CTA copies one slice,
+// or two where its share straddles a panel boundary.  CTAs take units from a
+// global counter and, inside a piece, warps take chunks from a shared counter.  Every segment's sum has one writer, so
+// which CTA or warp runs a chunk changes nothing in the results, and the SMs
+// finish together whatever the estimate of a unit's cost was worth.
 #pragma once
 #include "nk_device.cuh"
 #include <cuda_runtime.h>
@@ -31,8 +43,11 @@
 #ifndef NK_PANEL_THREADS
 #define NK_PANEL_THREADS 1024 // threads per CTA of panel_kernel (one CTA per SM)
 #endif
+#ifndef NK_PANEL_MIN_RUN
+#define NK_PANEL_MIN_RUN 32 // panels only when long rows average this many entries per panel
+#endif
 #ifndef NK_PANEL_UNROLL
-#define NK_PANEL_UNROLL 4
+#define NK_PANEL_UNROLL 8 // entries of its stream a lane loads before adding them
 #endif
 
 namespace nk {
@@ -40,65 +55,110 @@ namespace nk {
 constexpr int kPanelThreads = NK_PANEL_THREADS;
 constexpr int kPanelWarps = kPanelThreads / 32;
 constexpr int kPanelMinBlocks = 1024 / kPanelThreads;
+constexpr uint16_t kPanelMarker = 0xFFFF; // column of a segment's closing marker
+constexpr int64_t kPanelMaxWidth = 65535;  // columns 0 .. 0xFFFE
 
 template <class V> struct PanelView {
     int64_t rows = 0;        // long rows: engine rows [0, rows)
     int64_t cols = 0;        // columns of A
     int64_t width = 0;       // columns per panel (a multiple of 16)
-    const int64_t *uoff = nullptr; // CTA b runs units[uoff[b] .. uoff[b+1])
-    const int4 *units = nullptr;   // {panel, first chunk, end chunk, 0}
-    const int64_t *cptr = nullptr; // chunk c: entries [cptr[c], cptr[c+1])
-    const int2 *lane = nullptr;    // 32 per chunk: {row (-1: padding), entries}
-    const uint16_t *lidx = nullptr; // column within the panel
-    const V *val = nullptr;
+    int64_t nunits = 0;
+    const int4 *units = nullptr;   // pieces {panel, first chunk, end chunk, unit}
+    const int64_t *uoff = nullptr; // unit u: pieces [uoff[u], uoff[u+1])
+    const int64_t *cptr = nullptr; // chunk c: entries [cptr[c], cptr[c+1]), 32 per step
+    const uint16_t *lidx = nullptr; // column within the panel, or kPanelMarker
+    const V *val = nullptr;         // value, or at a marker the row (bits of an int)
     double *partial = nullptr;     // [panels][rows]
+    unsigned *claim = nullptr;     // [0] next unit, [1] CTAs done; zero between launches
 };
 
+// The row a marker's value slot carries.
+template <class V> __device__ __forceinline__ int64_t marker_row(V a) {
+    if constexpr (sizeof(V) == 8)
+        return int64_t(__double_as_longlong(double(a)));
+    else
+        return int64_t(__float_as_int(float(a)));
+}
+
 // One launch per trial, after primal_kernel (which writes dx) and before
-// dual_kernel (which adds the partials).  Grid: one CTA per unit list.
+// dual_kernel (which adds the partials).  Persistent grid, one CTA per SM.
 template <class Acc, class V, class X>
 __global__ void __launch_bounds__(kPanelThreads, kPanelMinBlocks)
     panel_kernel(PanelView<V> P, const X *__restrict__ dx, const Control *ctl) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
+    __shared__ unsigned unit, next_chunk;
     X *sdx = reinterpret_cast<X *>(dyn_smem);
-    if (ctl->restart != 0) // a requested Halpern restart freezes the chunk
+    if (ctl->restart != 0) // a requested Halpern restart freezes the chunk: no claims
         return;
-    const int warp = threadIdx.x >> 5, t = threadIdx.x & 31;
-    const int64_t u0 = P.uoff[blockIdx.x], u1 = P.uoff[blockIdx.x + 1];
-    for (int64_t u = u0; u < u1; ++u) {
-        const int4 w = P.units[u];
-        const int64_t col0 = int64_t(w.x) * P.width;
-        const int64_t cols = P.cols - col0 < P.width ? P.cols - col0 : P.width;
-        if (u > u0)
-            __syncthreads(); // every warp is done with the previous slice
-        stage16<kPanelThreads>(sdx, dx + col0, cols * int64_t(sizeof(X)));
+    const int t = threadIdx.x & 31;
+    for (;;) {
+        if (threadIdx.x == 0)
+            unit = atomicAdd(P.claim, 1u);
         __syncthreads();
-        double *out = P.partial + int64_t(w.x) * P.rows;
-        for (int64_t c = w.y + warp; c < w.z; c += kPanelWarps) {
-            const int2 rl = P.lane[c * 32 + t];
-            const int64_t base = P.cptr[c] + t;
-            const uint16_t *ip = P.lidx + base;
-            const V *vp = P.val + base;
-            Acc acc = Acc(0);
-            int k = 0;
-            constexpr int U = NK_PANEL_UNROLL;
-            for (; k + U <= rl.y; k += U) {
-                uint16_t j[U];
-                V a[U];
+        const unsigned u = unit;
+        if (u >= P.nunits)
+            break; // the whole CTA
+        for (int64_t pc = P.uoff[u]; pc < P.uoff[u + 1]; ++pc) {
+            const int4 w = P.units[pc];
+            if (threadIdx.x == 0)
+                next_chunk = 0;
+            const int64_t col0 = int64_t(w.x) * P.width;
+            const int64_t cols = P.cols - col0 < P.width ? P.cols - col0 : P.width;
+            stage16<kPanelThreads>(sdx, dx + col0, cols * int64_t(sizeof(X)));
+            __syncthreads();
+            double *out = P.partial + int64_t(w.x) * P.rows;
+            const int span = w.z - w.y;
+            for (;;) {
+                unsigned k = 0;
+                if (t == 0)
+                    k = atomicAdd(&next_chunk, 1u);
+                k = __shfl_sync(0xffffffffu, k, 0);
+                if (int(k) >= span)
+                    break;
+                const int64_t c = int64_t(w.y) + k;
+                const int64_t base = P.cptr[c] + t;
+                const int len = int((P.cptr[c + 1] - P.cptr[c]) >> 5);
+                const uint16_t *ip = P.lidx + base;
+                const V *vp = P.val + base;
+                Acc acc = Acc(0);
+                int e = 0;
+                constexpr int U = NK_PANEL_UNROLL;
+                for (; e + U <= len; e += U) {
+                    uint16_t j[U];
+                    V a[U];
 #pragma unroll
-                for (int q = 0; q < U; ++q) {
-                    j[q] = stream_load(ip + int64_t(k + q) * 32);
-                    a[q] = stream_load(vp + int64_t(k + q) * 32);
+                    for (int q = 0; q < U; ++q) {
+                        j[q] = stream_load(ip + int64_t(e + q) * 32);
+                        a[q] = stream_load(vp + int64_t(e + q) * 32);
+                    }
+#pragma unroll
+                    for (int q = 0; q < U; ++q) {
+                        if (j[q] == kPanelMarker) {
+                            out[marker_row(a[q])] = double(acc);
+                            acc = Acc(0);
+                        } else
+                            acc = acc + Acc(a[q]) * Acc(sdx[j[q]]);
+                    }
                 }
-#pragma unroll
-                for (int q = 0; q < U; ++q)
-                    acc = acc + Acc(a[q]) * Acc(sdx[j[q]]);
+                for (; e < len; ++e) {
+                    const uint16_t j = stream_load(ip + int64_t(e) * 32);
+                    const V a = stream_load(vp + int64_t(e) * 32);
+                    if (j == kPanelMarker) {
+                        out[marker_row(a)] = double(acc);
+                        acc = Acc(0);
+                    } else
+                        acc = acc + Acc(a) * Acc(sdx[j]);
+                }
             }
-            for (; k < rl.y; ++k)
-                acc = acc + Acc(stream_load(vp + int64_t(k) * 32)) *
-                                Acc(sdx[stream_load(ip + int64_t(k) * 32)]);
-            if (rl.x >= 0)
-                out[rl.x] = double(acc);
+            __syncthreads(); // the slice and the chunk counter are free for the next piece
+        }
+        __syncthreads(); // every thread has read `unit` (a unit may hold no piece)
+    }
+    if (threadIdx.x == 0) { // the last CTA out clears the counters for the next launch
+        __threadfence();
+        if (atomicAdd(P.claim + 1, 1u) == gridDim.x - 1) {
+            P.claim[0] = 0;
+            P.claim[1] = 0;
         }
     }
 }

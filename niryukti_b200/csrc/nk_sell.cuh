@@ -45,69 +45,17 @@ template <class V, class I> struct Sell {
                            //   segments, counter (-1: the row lies in one chunk)}
     double *slots;         // per split segment: partial sum
     unsigned *counters;    // per split row: arrivals (reset by the last one)
-    // Balanced warp schedule of the fused kernels (null: round-robin): the
-    // chunks of persistent warp w are wlist[woff[w] .. woff[w+1]).
-    const int64_t *woff = nullptr;
-    const int64_t *wlist = nullptr;
+    // The fused kernels' schedule: CTA b owns chunks clist[coff[b] .. coff[b+1]).
+    const int64_t *coff = nullptr;
+    const int64_t *clist = nullptr;
 };
-
-// Iterates the SELL chunks of the calling warp: the balanced schedule when the
-// matrix carries one (the grid it was built for), else round-robin over the
-// persistent grid.  Every lane of a warp sees the same chunks.
-template <class V, class I> struct WarpChunks {
-    const Sell<V, I> &M;
-    int64_t k, end, stride;
-    __device__ __forceinline__ explicit WarpChunks(const Sell<V, I> &m) : M(m) {
-        const int64_t w = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-        if (M.woff) {
-            k = M.woff[w];
-            end = M.woff[w + 1];
-            stride = 1;
-        } else {
-            k = w;
-            end = (M.nv + 31) >> 5;
-            stride = (int64_t(gridDim.x) * blockDim.x) >> 5;
-        }
-    }
-    __device__ __forceinline__ bool next(int64_t *ch) {
-        if (k >= end)
-            return false;
-        *ch = M.woff ? M.wlist[k] : k;
-        k += stride;
-        return true;
-    }
-};
-
-// One gathered entry x[j]: from the CTA's shared-memory copy of x[0, nhot)
-// when HOT and j lies there, else from global memory (flavour G).
-#ifndef NK_HOT_SELECT
-#define NK_HOT_SELECT 1 // 1: one generic load through a selected pointer, 0: a branch
-#endif
-template <int G, bool HOT, class X, class I>
-__device__ __forceinline__ X gather_entry(const X *__restrict__ x, I j, const X *hot,
-                                          int64_t nhot) {
-    if constexpr (HOT) {
-#if NK_HOT_SELECT
-        const X *p = int64_t(j) < nhot ? hot + j : x + j; // shared or global, per lane
-        return *p;
-#else
-        if (int64_t(j) < nhot)
-            return hot[j];
-#endif
-    }
-    return gather_as<G>(x + j);
-}
 
 // Sequential dot product of virtual row v (entries in CSR order) starting
 // from acc; U entries' loads are issued before their products are added.
-// Used inside the fused PDHG kernels, where registers are scarce.  With HOT,
-// entries below nhot are read from `hot`, a shared-memory copy of x[0, nhot):
-// a gather from shared memory costs the SM's load path a few bank cycles
-// where a scattered global load costs it a cache-line lookup of its own.
-template <class Acc, int U = kUnroll, int G = 0, bool HOT = false, class V, class I, class X>
+// Used inside the fused PDHG kernels, where registers are scarce.
+template <class Acc, int U = kUnroll, int G = 0, class V, class I, class X>
 __device__ __forceinline__ Acc sell_dot(const Sell<V, I> &M, int64_t v, int len, Acc acc,
-                                        const X *__restrict__ x, const X *hot = nullptr,
-                                        int64_t nhot = 0) {
+                                        const X *__restrict__ x) {
     const int64_t base = M.cptr[v >> 5] + (v & 31);
     const I *ip = M.idx + base;
     const V *vp = M.val + base;
@@ -123,14 +71,14 @@ __device__ __forceinline__ Acc sell_dot(const Sell<V, I> &M, int64_t v, int len,
         X g[U];
 #pragma unroll
         for (int u = 0; u < U; ++u)
-            g[u] = gather_entry<G, HOT>(x, j[u], hot, nhot);
+            g[u] = gather_as<G>(x + j[u]);
 #pragma unroll
         for (int u = 0; u < U; ++u)
             acc = acc + Acc(w[u]) * Acc(g[u]);
     }
     for (; k < len; ++k)
         acc = acc + Acc(stream_load(vp + int64_t(k) * 32)) *
-                        Acc(gather_entry<G, HOT>(x, stream_load(ip + int64_t(k) * 32), hot, nhot));
+                        Acc(gather_as<G>(x + stream_load(ip + int64_t(k) * 32)));
     return acc;
 }
 
