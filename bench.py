@@ -768,9 +768,11 @@ def synth_pool(args):
 # ---------------------------------------------------------------- engine arm
 S_V = {"fp64": 8, "mixed": 4, "fp32": 4}
 # DRAM bytes (read + write) per launch of each step of the power-law LP at
-# scale 0.5 from one ncu capture of the current kernels (the capture is named in
-# profiles/); the dual step is the panel kernel plus the dual kernel
-HALF_SCALE_TRAFFIC = {}
+# scale 0.5 from one ncu capture of the current kernels
+# (profiles/fused_pdhg_kernels_power_law_lp_half_scale.md); on this LP the dual
+# step is the dual kernel alone (its long rows average fewer than 32 entries
+# per column panel, so they take no panel kernel)
+HALF_SCALE_TRAFFIC = {"primal_kernel": 168.526e6 + 5.193e6, "dual_step": 162.280e6 + 4.179e6}
 
 
 def step_kernels(g, model, s_v, trials, tau, sigma):
