@@ -557,10 +557,11 @@ def batch_models(args):
 
 def batch_section(args):
     """The batch: 512 uneven LP/QP instances (m log-uniform in [500, 50000],
-    n = 2m, 20% QPs) solved to 1e-6 relative KKT by the batched engine (FP32
-    matrices, FP64 iterates and reductions), beside the plain FP64 solve run
-    instance by instance on the same GPU (a stratified sample, timed one by
-    one) and the reference's CPU solve of the same sample."""
+    n = 2m, 20% QPs) solved to 1e-6 relative KKT by the batched engine
+    (--batch-precision: FP64, or MIXED with FP32 matrices and FP64 iterates and
+    reductions), beside the plain FP64 solve run instance by instance on the same
+    GPU (a stratified sample, timed one by one) and the reference's CPU solve of
+    the same sample."""
     from concurrent.futures import ThreadPoolExecutor
     from niryukti_b200 import batch as nb, solver
     t0 = time.perf_counter()
@@ -681,8 +682,9 @@ def batch_throughput(args):
 def serve_section(args):
     """The served stream: Poisson arrivals at --serve-rate requests/s for --serve-seconds,
     each request drawn from a pool of instances of the uneven LP/QP mix with m
-    log-uniform in [500, 200000]; served by continuous batching (admission by
-    device-memory footprint under a 150 GB budget), and by the plain FP64
+    log-uniform in [500, 200000]; served by continuous batching at
+    --serve-precision (admission by device-memory footprint under a 150 GB
+    budget), and by the plain FP64
     solve one request at a time on the same arrival stream.  Reported over the
     arrival window plus a drain of --serve-drain seconds: completed solves per
     second and the latency percentiles of the completed requests; requests
@@ -707,7 +709,7 @@ def serve_section(args):
                 "p99_s": pct(.99)}
 
     # served: a feeder submits at the arrival times
-    svc = serve.SolveService(memory_budget=150e9, matrix_precision="mixed",
+    svc = serve.SolveService(memory_budget=150e9, matrix_precision=args.serve_precision,
                              prepare_workers=os.cpu_count() or 8,
                              iteration_limit=100000, time_limit=horizon,
                              max_active_nnz=int(args.serve_active_nnz))
@@ -1093,7 +1095,10 @@ def main():
                     help="work cap of the running batch (nonzeros)")
     ap.add_argument("--batch-m-hi", type=int, default=50000)
     ap.add_argument("--batch-sample", type=int, default=16)
-    ap.add_argument("--batch-precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--batch-precision", default="fp64", choices=["fp64", "mixed"],
+                    help="matrix precision of the batch")
+    ap.add_argument("--serve-precision", default="mixed", choices=["fp64", "mixed"],
+                    help="matrix precision of the served stream")
     ap.add_argument("--batch-cpu-sample", type=int, default=4,
                     help="smallest sampled instances also solved by the reference on the CPU")
     ap.add_argument("--no-forms", action="store_true",

@@ -132,10 +132,12 @@ nk_status nk_pdhg_profile_kernels(nk_pdhg *h, int count, double tau, double sigm
                                   double ms[3]);
 /* Layout of the dual SpMV (no reference counterpart): how many of A's rows
  * (its longest, past the SELL split length) are stored by column panel, the
- * panel width in columns, the number of panels (all 0 without panels), and
- * the kernel launches per trial.  Null outputs are skipped. */
+ * panel width in columns, the number of panels, the number of runs (a long
+ * row's entries in one panel, cut into pieces of 64 or more entries where
+ * they would hold up a lane; each run has its own partial sum) (all 0 without
+ * panels), and the kernel launches per trial.  Null outputs are skipped. */
 nk_status nk_pdhg_layout_info(nk_pdhg *h, int64_t *long_rows, int64_t *panel_width,
-                              int *panels, int *kernels_per_trial);
+                              int *panels, int64_t *runs, int *kernels_per_trial);
 /* Profiling (no reference counterpart): mean duration in milliseconds of `reps`
  * plain SpMVs (no fused epilogue) with A (which = 0, input x) or A^T (which = 1,
  * input y) on the resident iterate; results go to scratch, iterates unchanged. */
@@ -275,7 +277,7 @@ typedef struct {
     int check_every;          /* trials between candidate checks (100) */
     int presolve, scaling_combined, scaling_passes, adaptive, restart, graphs;
     int autotune;             /* time kernel variants on the live batch (1) */
-    int precision;            /* NK_PRECISION_FP64, or MIXED (the default): FP32 values
+    int precision;            /* NK_PRECISION_FP64 (the default), or MIXED: FP32 values
                                  until an instance's KKT reaches phase_tol or stalls,
                                  then an FP64 refinement restarted from its best point */
     double phase_tol;         /* MIXED phase target (0: 10 * tol) */

@@ -58,7 +58,7 @@ def _bind():
 
 def batch_options(*, tol=1e-6, time_limit=60.0, iteration_limit=100000, check_every=100,
                   presolve=True, scaling="ruiz", scaling_passes=5, adaptive=True, restart=True,
-                  cuda_graphs=True, autotune=True, matrix_precision="mixed", phase_tol=0.0,
+                  cuda_graphs=True, autotune=True, matrix_precision="fp64", phase_tol=0.0,
                   memory_budget=0.0, capacity=4096) -> NkBatchOptions:
     L = _bind()
     if scaling not in ("ruiz", "combined"):
@@ -108,7 +108,7 @@ class BatchEngine:
 
     def __init__(self, **options):
         self._L = _bind()
-        self.precision = options.get("matrix_precision", "mixed")
+        self.precision = options.get("matrix_precision", "fp64")
         self.options = batch_options(**options)
         self._h = C.c_void_p()
         check(self._L.nk_batch_create(C.byref(self.options), C.byref(self._h)))

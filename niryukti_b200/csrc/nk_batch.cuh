@@ -25,7 +25,7 @@ struct BatchOptions {
     int check_every = 100;
     PrepareOptions prepare;
     bool adaptive = true, restart = true, graphs = true, autotune = true;
-    int precision = NK_PRECISION_MIXED;
+    int precision = NK_PRECISION_FP64;
     double phase_tol = 0;     // MIXED: KKT at which an instance moves to FP64 (0: 10 * tol)
     double memory_budget = 0; // bytes; 0: 80% of the free device memory at creation
     int capacity = 4096;
@@ -1216,6 +1216,14 @@ class Batch {
                 for (int e = 0; e < 9; ++e, level /= 10)
                     if (S.best.kkt <= level && S.reached[e] < 0)
                         S.reached[e] = since(S.start);
+            }
+            if ((S.empty >= 4 || !ca.finite) && !S.fp64_phase && S.best.finite) {
+                // stalled backtracking or a nonfinite candidate on the FP32 values
+                // ends the reduced-precision phase: FP64 refinement restarts from
+                // the best point
+                S.empty = 0;
+                refine_on.push_back(b);
+                continue;
             }
             if (S.empty >= 4) {
                 retire(S, NK_SOLVE_NUMERICAL_ERROR);

@@ -83,8 +83,10 @@ struct Vecs {
     double *split_p;      // [At's cross-chunk split rows]
     double *split_d;      // [2 * A's cross-chunk split rows]
     int nsplit_p, nsplit_d;
-    // panel path of A's long rows (nk_panel.cuh): partial[p * panel_rows + i]
+    // panel path of A's long rows (nk_panel.cuh): long row i's run sums are
+    // panel_partial[panel_roff[i] .. panel_roff[i+1])
     const double *panel_partial;
+    const int64_t *panel_roff;
     int64_t panel_rows;
     int npanels;
 };
@@ -432,9 +434,10 @@ __device__ inline void decide(Vecs &v, double p, double d, double c) {
 }
 
 // PANEL: A's long rows (engine rows [0, v.panel_rows)) come from panel_kernel
-// as one partial sum per column panel; the schedule lists them as "combine
-// chunks" (encoded -k-1 for rows [32k, 32k+32)) in place of their split-row
-// chunks, and a lane adds its row's partials in panel order.
+// as one partial sum per run (a row's entries in one column panel, or a cut
+// of them); the schedule lists them as "combine chunks" (encoded -k-1 for
+// rows [32k, 32k+32)) in place of their split-row chunks, and a lane adds its
+// row's run sums in slot order (panel by panel, runs in CSR order).
 template <class Acc, class V, class I, bool FP32G, bool SPLIT, bool PANEL = false>
 __global__ void __launch_bounds__(kFusedThreads, kFusedMinBlocks)
     dual_kernel(Sell<V, I> A, Vecs v) {
@@ -485,28 +488,28 @@ __global__ void __launch_bounds__(kFusedThreads, kFusedMinBlocks)
             double dy2 = 0, cpl = 0;
             bool combine = false;
             if constexpr (PANEL) {
-                if (ch < 0) { // long rows: their panel partials, in panel order
+                if (ch < 0) { // long rows: their run sums, in slot order
                     combine = true;
                     const int64_t i = (-ch - 1) * 32 + lane;
                     if (i < v.panel_rows) {
                         const double yi = y[i], axi = ax[i], rli = v.rl[i], rui = v.ru[i];
                         const double ai = pending ? v.ya[i] : 0.;
-                        const double *pp = v.panel_partial + i;
-                        const int64_t stride = v.panel_rows;
+                        const int64_t s0 = v.panel_roff[i], s1 = v.panel_roff[i + 1];
+                        const double *pp = v.panel_partial;
                         double delta = 0;
-                        int p = 0;
-                        constexpr int B = 8; // loads in flight; the adds stay in panel order
-                        for (; p + B <= v.npanels; p += B) {
+                        int64_t p = s0;
+                        constexpr int B = 8; // loads in flight; the adds stay in slot order
+                        for (; p + B <= s1; p += B) {
                             double a[B];
 #pragma unroll
                             for (int q = 0; q < B; ++q)
-                                a[q] = __ldcg(pp + (p + q) * stride);
+                                a[q] = __ldcg(pp + p + q);
 #pragma unroll
                             for (int q = 0; q < B; ++q)
                                 delta += a[q];
                         }
-                        for (; p < v.npanels; ++p)
-                            delta += __ldcg(pp + p * stride);
+                        for (; p < s1; ++p)
+                            delta += __ldcg(pp + p);
                         finish(i, delta, yi, axi, rli, rui, ai, dy2, cpl);
                     }
                 }

@@ -12,26 +12,28 @@
 // (a few bank cycles per warp instead of one lookup per lane).
 //
 // Inside a panel each row with entries there is a segment: its entries in CSR
-// order followed by a marker entry (column 0xFFFF) whose value slot carries
-// the row's index.  Segments are packed whole into lanes, longest first onto
-// the least-loaded lane, so every lane holds a stream of nearly the same
-// length.
+// order.  A segment longer than a quarter of a lane's expected stream is cut
+// into runs of nearly equal length; a shorter one is one run.  Each run is
+// followed by a marker entry (column 0xFFFF) whose value slot carries the run's
+// slot number, and runs are packed whole into lanes, longest first onto the
+// least-loaded lane, so every lane holds a stream of nearly the same length.
 // A chunk's 32 lane streams are stored column-major as in SELL-32 (entry k of
-// lane t of chunk c at cptr[c] + 32*k + t).  A lane adds its entries one by one; at a marker
-// it writes the sum to partial[p*rows + row] and starts again from zero.  So a
-// row's panel sum is its sequential CSR sum over that panel, and no lane waits
-// on a lookup: the row number arrives in the stream.  (row, panel) pairs
-// without entries are never written and stay zero.  The dual kernel then adds
-// a long row's partials in panel order 0, 1, ..., from zero: the result does
-// not depend on timing, and with a single panel it is the row's sequential CSR
-// sum, the CPU's order.
+// lane t of chunk c at cptr[c] + 32*k + t).  A lane adds its entries one by
+// one; at a marker it writes the sum to partial[slot] and starts again from
+// zero.  So a run's sum is its sequential CSR sum, and no lane waits on a
+// lookup: the slot number arrives in the stream.  Slots are numbered row by
+// row, then by panel, then by run, so long row i owns slots
+// [roff[i], roff[i+1]); the dual kernel adds them in that order from zero.
+// The result does not depend on timing, and for a row held by one run (one
+// panel, not cut) it is the row's sequential CSR sum, the CPU's order.
 //
 // A unit is an equal share of all panels' entries, one per CTA; it holds one
 // piece (one chunk per warp) per panel it touches, so a CTA copies one slice,
 // or two where its share straddles a panel boundary.  CTAs take units from a
-// global counter and, inside a piece, warps take chunks from a shared counter.  Every segment's sum has one writer, so
-// which CTA or warp runs a chunk changes nothing in the results, and the SMs
-// finish together whatever the estimate of a unit's cost was worth.
+// global counter and, inside a piece, warps take chunks from a shared counter.
+// Every run's sum has one writer, so which CTA or warp runs a chunk changes
+// nothing in the results, and the SMs finish together whatever the estimate
+// of a unit's cost was worth.
 #pragma once
 #include "nk_device.cuh"
 #include <cuda_runtime.h>
@@ -45,6 +47,9 @@
 #endif
 #ifndef NK_PANEL_MIN_RUN
 #define NK_PANEL_MIN_RUN 32 // panels only when long rows average this many entries per panel
+#endif
+#ifndef NK_PANEL_MIN_SPLIT
+#define NK_PANEL_MIN_SPLIT 64 // segments are cut into runs of no fewer entries than this
 #endif
 #ifndef NK_PANEL_UNROLL
 #define NK_PANEL_UNROLL 8 // entries of its stream a lane loads before adding them
@@ -67,13 +72,14 @@ template <class V> struct PanelView {
     const int64_t *uoff = nullptr; // unit u: pieces [uoff[u], uoff[u+1])
     const int64_t *cptr = nullptr; // chunk c: entries [cptr[c], cptr[c+1]), 32 per step
     const uint16_t *lidx = nullptr; // column within the panel, or kPanelMarker
-    const V *val = nullptr;         // value, or at a marker the row (bits of an int)
-    double *partial = nullptr;     // [panels][rows]
+    const V *val = nullptr;         // value, or at a marker the slot (bits of an int)
+    double *partial = nullptr;     // one per slot
+    int64_t slots = 0;
     unsigned *claim = nullptr;     // [0] next unit, [1] CTAs done; zero between launches
 };
 
-// The row a marker's value slot carries.
-template <class V> __device__ __forceinline__ int64_t marker_row(V a) {
+// The slot a marker's value carries.
+template <class V> __device__ __forceinline__ int64_t marker_slot(V a) {
     if constexpr (sizeof(V) == 8)
         return int64_t(__double_as_longlong(double(a)));
     else
@@ -106,7 +112,7 @@ __global__ void __launch_bounds__(kPanelThreads, kPanelMinBlocks)
             const int64_t cols = P.cols - col0 < P.width ? P.cols - col0 : P.width;
             stage16<kPanelThreads>(sdx, dx + col0, cols * int64_t(sizeof(X)));
             __syncthreads();
-            double *out = P.partial + int64_t(w.x) * P.rows;
+            double *out = P.partial;
             const int span = w.z - w.y;
             for (;;) {
                 unsigned k = 0;
@@ -134,7 +140,9 @@ __global__ void __launch_bounds__(kPanelThreads, kPanelMinBlocks)
 #pragma unroll
                     for (int q = 0; q < U; ++q) {
                         if (j[q] == kPanelMarker) {
-                            out[marker_row(a[q])] = double(acc);
+                            const int64_t sl = marker_slot(a[q]);
+                            if (sl >= 0 && sl < P.slots) // a layout fault drops the sum
+                                out[sl] = double(acc);
                             acc = Acc(0);
                         } else
                             acc = acc + Acc(a[q]) * Acc(sdx[j[q]]);
@@ -144,7 +152,9 @@ __global__ void __launch_bounds__(kPanelThreads, kPanelMinBlocks)
                     const uint16_t j = stream_load(ip + int64_t(e) * 32);
                     const V a = stream_load(vp + int64_t(e) * 32);
                     if (j == kPanelMarker) {
-                        out[marker_row(a)] = double(acc);
+                        const int64_t sl = marker_slot(a);
+                        if (sl >= 0 && sl < P.slots)
+                            out[sl] = double(acc);
                         acc = Acc(0);
                     } else
                         acc = acc + Acc(a) * Acc(sdx[j]);

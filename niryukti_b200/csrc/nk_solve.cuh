@@ -854,7 +854,14 @@ inline SolveReport solve(const HostModel &original, const SolveSettings &S) {
     Accuracy best;
     if (phased) {
         double target = S.phase_tol > 0 ? S.phase_tol : 10 * o.tol;
-        drv.run(S.refine ? target : o.tol, !S.refine, o.iteration_limit);
+        try {
+            drv.run(S.refine ? target : o.tol, !S.refine, o.iteration_limit);
+        } catch (const Error &e) {
+            // backtracking that stalls on the reduced-precision values ends the
+            // phase: the FP64 refinement restarts from the best point
+            if (e.status != NK_ERR_STALLED || !S.refine || !drv.best.finite)
+                throw;
+        }
         best = drv.best;
         R.mixed_iterations = R.iterations;
         R.mixed_seconds = since(start);

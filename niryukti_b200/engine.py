@@ -75,7 +75,7 @@ def library() -> C.CDLL:
     L.nk_pdhg_stats.argtypes = [C.c_void_p, _I, _I]
     L.nk_pdhg_profile.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, _D, _D]
     L.nk_pdhg_profile_kernels.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, _D]
-    L.nk_pdhg_layout_info.argtypes = [C.c_void_p, _I, _I, C.POINTER(C.c_int),
+    L.nk_pdhg_layout_info.argtypes = [C.c_void_p, _I, _I, C.POINTER(C.c_int), _I,
                                       C.POINTER(C.c_int)]
     L.nk_pdhg_schedule_info.argtypes = [C.c_void_p, C.POINTER(C.c_int), _I, C.POINTER(C.c_int),
                                         _I, C.POINTER(C.c_int), C.POINTER(C.c_int)]
@@ -319,13 +319,14 @@ class PdhgBackend:
 
     def layout_info(self):
         """The dual SpMV's layout: long rows stored by column panel, the panel
-        width, the panel count and the kernel launches per trial."""
-        r, w = C.c_int64(), C.c_int64()
+        width, the panel count, the runs (partial sums) of the long rows and the
+        kernel launches per trial."""
+        r, w, n = C.c_int64(), C.c_int64(), C.c_int64()
         p, k = C.c_int(), C.c_int()
         check(self._L.nk_pdhg_layout_info(self._h, C.byref(r), C.byref(w), C.byref(p),
-                                          C.byref(k)))
+                                          C.byref(n), C.byref(k)))
         return {"panel_rows": r.value, "panel_width": w.value, "panels": p.value,
-                "kernels_per_trial": k.value}
+                "panel_runs": n.value, "kernels_per_trial": k.value}
 
     def time_spmv(self, which: str, reps: int = 20) -> float:
         """Mean ms of a plain SpMV with A ("A") or A^T ("At") on the resident iterate."""
