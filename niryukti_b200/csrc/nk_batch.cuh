@@ -398,6 +398,19 @@ class Batch {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev);
+        const void *kernels[] = {(const void *)batch_primal<2>, (const void *)batch_primal<4>,
+                                 (const void *)batch_primal<8>, (const void *)batch_dual<2>,
+                                 (const void *)batch_dual<4>, (const void *)batch_dual<8>};
+        for (int t = 0; t < kCtaSizes; ++t) {
+            int least = 1 << 30;
+            for (const void *k : kernels) {
+                int per = 1;
+                cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, kCtaSize[t], 0),
+                           "occupancy");
+                least = std::min(least, per);
+            }
+            resident_[t] = std::max(1, least);
+        }
     }
     ~Batch() {
         if (stream_)
@@ -590,8 +603,17 @@ class Batch {
     DevBuf<int2> d_cols_, d_rows_;     // instance-contiguous (element kernels, partial layout)
     static constexpr int kRunLengths = 3;
     static constexpr int kRunLength[kRunLengths] = {1, 4, 16};
-    DevBuf<BWork> d_wcols_[kRunLengths], d_wrows_[kRunLengths]; // trial items, costliest first
-    int nwc_[kRunLengths] = {}, nwr_[kRunLengths] = {};
+    static constexpr int kCtaSizes = 3;
+    static constexpr int kCtaSize[kCtaSizes] = {128, 256, 512};
+    // trial items of each (run length, CTA size): per-CTA lists, CTA b's items
+    // [coff[b], coff[b+1]) costliest first, over a resident grid of ncta CTAs
+    struct WorkList {
+        DevBuf<BWork> items;
+        DevBuf<int> coff;
+        int count = 0, ncta = 0;
+    };
+    WorkList wcols_[kRunLengths][kCtaSizes], wrows_[kRunLengths][kCtaSizes];
+    int resident_[kCtaSizes] = {}; // CTAs of each size one SM holds (every variant)
     DevBuf<double> d_pp_, d_pd_, d_pk_, d_out_;
     BCtl *h_ctl_ = nullptr;
     int *h_mask_ = nullptr, *h_src_ = nullptr;
@@ -779,11 +801,11 @@ class Batch {
             trial_bytes_ += 2 * (nnz * (vb + 4) + 4 * (B.m + B.n)) + 8 * (B.m + B.n);
         }
         // trial work lists for each run length K: runs of K consecutive chunks
-        // of one instance, costliest first, so that the persistent warps'
-        // round-robin gives every warp a similar share (longest-first greedy)
+        // of one instance with their estimated cost, costliest first
+        // (a stable counting sort)
         auto runs = [&](const std::vector<int2> &list, const std::vector<int64_t> &cost,
-                        const std::vector<int> &first, const std::vector<int> &count, int K) {
-            // items with their costs, then a stable counting sort, costliest first
+                        const std::vector<int> &first, const std::vector<int> &count, int K,
+                        std::vector<int64_t> &sorted_cost) {
             std::vector<BWork> items;
             std::vector<int64_t> icost;
             int64_t top = 0;
@@ -804,28 +826,61 @@ class Batch {
             for (size_t b = 1; b < start.size(); ++b)
                 start[b] += start[b - 1];
             std::vector<BWork> out(items.size());
-            for (size_t k = 0; k < items.size(); ++k)
-                out[size_t(start[size_t(top - icost[k])]++)] = items[k];
+            sorted_cost.assign(items.size(), 0);
+            for (size_t k = 0; k < items.size(); ++k) {
+                const size_t at = size_t(start[size_t(top - icost[k])]++);
+                out[at] = items[k];
+                sorted_cost[at] = icost[k];
+            }
             return out;
         };
-        auto upload_list = [&](DevBuf<BWork> &d, const std::vector<BWork> &h) {
-            ensure(d, std::max<size_t>(1, h.size()));
-            if (!h.empty())
-                cuda_check(cudaMemcpy(d.p, h.data(), h.size() * sizeof(BWork), cudaMemcpyHostToDevice),
-                           "lists");
+        // items (costliest first) onto a resident grid of CTAs of size t, each
+        // onto the least-loaded CTA; a CTA's list keeps the costliest-first order
+        auto place = [&](WorkList &W, const std::vector<BWork> &items,
+                         const std::vector<int64_t> &icost, int t) {
+            const int ncta = std::max(1, std::min<int>(int(items.size()), sms_ * resident_[t]));
+            using Load = std::pair<int64_t, int>;
+            std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+            for (int b = 0; b < ncta; ++b)
+                heap.push({0, b});
+            std::vector<int> owner(items.size());
+            std::vector<int> coff(size_t(ncta + 1), 0);
+            for (size_t k = 0; k < items.size(); ++k) {
+                Load l = heap.top();
+                heap.pop();
+                owner[k] = l.second;
+                ++coff[size_t(l.second + 1)];
+                heap.push({l.first + icost[k], l.second});
+            }
+            for (int b = 0; b < ncta; ++b)
+                coff[size_t(b + 1)] += coff[size_t(b)];
+            std::vector<BWork> out(std::max<size_t>(1, items.size()));
+            std::vector<int> fill(coff.begin(), coff.end() - 1);
+            for (size_t k = 0; k < items.size(); ++k)
+                out[size_t(fill[size_t(owner[k])]++)] = items[k];
+            ensure(W.items, out.size());
+            ensure(W.coff, coff.size());
+            cuda_check(cudaMemcpy(W.items.p, out.data(), out.size() * sizeof(BWork),
+                                  cudaMemcpyHostToDevice), "lists");
+            cuda_check(cudaMemcpy(W.coff.p, coff.data(), coff.size() * sizeof(int),
+                                  cudaMemcpyHostToDevice), "lists");
+            W.count = int(items.size());
+            W.ncta = ncta;
         };
         for (int r = 0; r < kRunLengths; ++r) {
-            // after tuning only the chosen run lengths are launched
-            const bool need_c = !tuned_ || r == vp_ / 9, need_r = !tuned_ || r == vd_ / 9;
-            if (need_c) {
-                auto wc = runs(cols, ccost, cf, cc, kRunLength[r]);
-                nwc_[r] = int(wc.size());
-                upload_list(d_wcols_[r], wc);
+            // after tuning only the chosen variants' lists are launched
+            std::vector<int64_t> cost;
+            if (!tuned_ || r == vp_ / 9) {
+                auto wc = runs(cols, ccost, cf, cc, kRunLength[r], cost);
+                for (int t = 0; t < kCtaSizes; ++t)
+                    if (!tuned_ || t == vp_ % 3)
+                        place(wcols_[r][t], wc, cost, t);
             }
-            if (need_r) {
-                auto wr = runs(rows, rcost, rf, rc, kRunLength[r]);
-                nwr_[r] = int(wr.size());
-                upload_list(d_wrows_[r], wr);
+            if (!tuned_ || r == vd_ / 9) {
+                auto wr = runs(rows, rcost, rf, rc, kRunLength[r], cost);
+                for (int t = 0; t < kCtaSizes; ++t)
+                    if (!tuned_ || t == vd_ % 3)
+                        place(wrows_[r][t], wr, cost, t);
             }
         }
         ncols_ = int(cols.size());
@@ -870,22 +925,18 @@ class Batch {
     // {2, 4, 8}[v / 3 % 3], CTA size {128, 256, 512}[v % 3]
     static constexpr int kVariants = 27;
     void launch_half(int v, bool primal, bool probe = false) {
-        static const int threads_of[3] = {128, 256, 512};
-        const int threads = threads_of[v % 3], u = v / 3 % 3, r = v / 9;
-        const int items = primal ? nwc_[r] : nwr_[r];
-        if (items == 0)
+        const int t = v % 3, u = v / 3 % 3, r = v / 9;
+        const WorkList &W = primal ? wcols_[r][t] : wrows_[r][t];
+        if (W.count == 0)
             return;
-        const int per_block = threads / 32;
-        const int grid = std::max(1, std::min((items + per_block - 1) / per_block,
-                                              sms_ * (2048 / threads)));
         if (primal) {
             auto *k = u == 0 ? batch_primal<2> : u == 1 ? batch_primal<4> : batch_primal<8>;
-            k<<<grid, threads, 0, stream_>>>(d_ins_.p, d_ctl_.p, d_wcols_[r].p, items, d_pp_.p,
-                                             int(probe));
+            k<<<W.ncta, kCtaSize[t], 0, stream_>>>(d_ins_.p, d_ctl_.p, W.items.p, W.coff.p,
+                                                   d_pp_.p, int(probe));
         } else {
             auto *k = u == 0 ? batch_dual<2> : u == 1 ? batch_dual<4> : batch_dual<8>;
-            k<<<grid, threads, 0, stream_>>>(d_ins_.p, d_ctl_.p, d_wrows_[r].p, items, d_pd_.p,
-                                             int(probe));
+            k<<<W.ncta, kCtaSize[t], 0, stream_>>>(d_ins_.p, d_ctl_.p, W.items.p, W.coff.p,
+                                                   d_pd_.p, int(probe));
         }
     }
     void launch_decide() {

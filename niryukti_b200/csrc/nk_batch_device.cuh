@@ -47,11 +47,31 @@ struct BCtl { // per instance; the first fields mirror Control (nk_device.cuh)
 
 // Work item of the trial kernels: a run of `count` consecutive chunks of one
 // instance starting at `chunk`, whose partial sums go to part, part+1, ...
-// (partials are instance-contiguous; items are ordered by estimated cost,
-// largest first, for balance).  A run shares one descriptor fetch.
+// (partials are instance-contiguous).  A run shares one descriptor fetch.
+// Items are placed on CTAs on the host by estimated memory work (longest
+// first onto the least-loaded CTA; CTA b owns list entries [coff[b],
+// coff[b+1]), costliest first), and a CTA's warps claim its items from a
+// shared counter, so every SM finishes its share at about the same time.
+// Where an item runs changes no result: its partials have fixed slots.
 struct BWork {
     int inst, chunk, part, count;
 };
+
+// CTA size bound of the trial kernels: every variant keeps 1024 threads of
+// one SM resident (64 registers a thread), so a grid of sms * 1024 / threads
+// CTAs is resident at once.
+constexpr int kBatchMaxThreads = 512;
+
+// The warp's next item of its CTA's list (lane 0 claims; false when the list
+// is done).
+__device__ __forceinline__ bool claim_item(unsigned *next, int count, int *w) {
+    unsigned k = 0;
+    if ((threadIdx.x & 31) == 0)
+        k = atomicAdd(next, 1u);
+    k = __shfl_sync(0xffffffffu, k, 0);
+    *w = int(k);
+    return int(k) < count;
+}
 
 // Sequential dot of row r of a SELL matrix (32-row chunks, column-major)
 // starting from acc; U loads in flight per lane.
@@ -135,13 +155,18 @@ __device__ __forceinline__ double chunk_q(const BInst &I, bool f64, int j, bool 
 // writes only the trial buffers, dx and the partials, which the next trial
 // overwrites, so it leaves no trace in any instance's trajectory.
 template <int U>
-__global__ void batch_primal(const BInst *__restrict__ ins, const BCtl *__restrict__ ctl,
-                             const BWork *__restrict__ work, int nwork, double *part,
-                             int probe) {
+__global__ void __launch_bounds__(kBatchMaxThreads, 1024 / kBatchMaxThreads)
+    batch_primal(const BInst *__restrict__ ins, const BCtl *__restrict__ ctl,
+                 const BWork *__restrict__ work, const int *__restrict__ coff, double *part,
+                 int probe) {
+    __shared__ unsigned next;
     const int lane = threadIdx.x & 31;
-    const int warps = int((int64_t(gridDim.x) * blockDim.x) >> 5);
-    for (int w = int((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5); w < nwork; w += warps) {
-        const BWork it = work[w];
+    const int begin = coff[blockIdx.x], count = coff[blockIdx.x + 1] - begin;
+    if (threadIdx.x == 0)
+        next = 0;
+    __syncthreads();
+    for (int w; claim_item(&next, count, &w);) {
+        const BWork it = work[begin + w];
         const BCtl &s = ctl[it.inst];
         if (!s.active) {
             if (lane < it.count)
@@ -188,12 +213,18 @@ __global__ void batch_primal(const BInst *__restrict__ ins, const BCtl *__restri
 // part[2 (w.part + k)] = sum dy^2, part[2 (w.part + k) + 1] = sum dy * delta.
 // `probe` as for batch_primal.
 template <int U>
-__global__ void batch_dual(const BInst *__restrict__ ins, const BCtl *__restrict__ ctl,
-                           const BWork *__restrict__ work, int nwork, double *part, int probe) {
+__global__ void __launch_bounds__(kBatchMaxThreads, 1024 / kBatchMaxThreads)
+    batch_dual(const BInst *__restrict__ ins, const BCtl *__restrict__ ctl,
+               const BWork *__restrict__ work, const int *__restrict__ coff, double *part,
+               int probe) {
+    __shared__ unsigned next;
     const int lane = threadIdx.x & 31;
-    const int warps = int((int64_t(gridDim.x) * blockDim.x) >> 5);
-    for (int w = int((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5); w < nwork; w += warps) {
-        const BWork it = work[w];
+    const int begin = coff[blockIdx.x], count = coff[blockIdx.x + 1] - begin;
+    if (threadIdx.x == 0)
+        next = 0;
+    __syncthreads();
+    for (int w; claim_item(&next, count, &w);) {
+        const BWork it = work[begin + w];
         const BCtl &s = ctl[it.inst];
         if (!s.active) {
             if (lane < it.count) {
