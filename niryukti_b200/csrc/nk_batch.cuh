@@ -801,11 +801,10 @@ class Batch {
             trial_bytes_ += 2 * (nnz * (vb + 4) + 4 * (B.m + B.n)) + 8 * (B.m + B.n);
         }
         // trial work lists for each run length K: runs of K consecutive chunks
-        // of one instance with their estimated cost, costliest first
-        // (a stable counting sort)
+        // of one instance, costliest first by estimated cost (a stable
+        // counting sort)
         auto runs = [&](const std::vector<int2> &list, const std::vector<int64_t> &cost,
-                        const std::vector<int> &first, const std::vector<int> &count, int K,
-                        std::vector<int64_t> &sorted_cost) {
+                        const std::vector<int> &first, const std::vector<int> &count, int K) {
             std::vector<BWork> items;
             std::vector<int64_t> icost;
             int64_t top = 0;
@@ -826,31 +825,23 @@ class Batch {
             for (size_t b = 1; b < start.size(); ++b)
                 start[b] += start[b - 1];
             std::vector<BWork> out(items.size());
-            sorted_cost.assign(items.size(), 0);
-            for (size_t k = 0; k < items.size(); ++k) {
-                const size_t at = size_t(start[size_t(top - icost[k])]++);
-                out[at] = items[k];
-                sorted_cost[at] = icost[k];
-            }
+            for (size_t k = 0; k < items.size(); ++k)
+                out[size_t(start[size_t(top - icost[k])]++)] = items[k];
             return out;
         };
-        // items (costliest first) onto a resident grid of CTAs of size t, each
-        // onto the least-loaded CTA; a CTA's list keeps the costliest-first order
-        auto place = [&](WorkList &W, const std::vector<BWork> &items,
-                         const std::vector<int64_t> &icost, int t) {
+        // items (costliest first) onto a resident grid of CTAs of size t, dealt
+        // in rounds of one item per CTA, alternating direction (round k deals
+        // to CTAs 0..G-1 when k is even, G-1..0 when odd): with items sorted by
+        // cost this balances estimated work like longest-first placement, in
+        // linear time.  A CTA's list keeps the costliest-first order.
+        auto place = [&](WorkList &W, const std::vector<BWork> &items, int t) {
             const int ncta = std::max(1, std::min<int>(int(items.size()), sms_ * resident_[t]));
-            using Load = std::pair<int64_t, int>;
-            std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
-            for (int b = 0; b < ncta; ++b)
-                heap.push({0, b});
             std::vector<int> owner(items.size());
             std::vector<int> coff(size_t(ncta + 1), 0);
             for (size_t k = 0; k < items.size(); ++k) {
-                Load l = heap.top();
-                heap.pop();
-                owner[k] = l.second;
-                ++coff[size_t(l.second + 1)];
-                heap.push({l.first + icost[k], l.second});
+                const int round = int(k / size_t(ncta)), at = int(k % size_t(ncta));
+                owner[k] = round % 2 ? ncta - 1 - at : at;
+                ++coff[size_t(owner[k] + 1)];
             }
             for (int b = 0; b < ncta; ++b)
                 coff[size_t(b + 1)] += coff[size_t(b)];
@@ -869,18 +860,17 @@ class Batch {
         };
         for (int r = 0; r < kRunLengths; ++r) {
             // after tuning only the chosen variants' lists are launched
-            std::vector<int64_t> cost;
             if (!tuned_ || r == vp_ / 9) {
-                auto wc = runs(cols, ccost, cf, cc, kRunLength[r], cost);
+                auto wc = runs(cols, ccost, cf, cc, kRunLength[r]);
                 for (int t = 0; t < kCtaSizes; ++t)
                     if (!tuned_ || t == vp_ % 3)
-                        place(wcols_[r][t], wc, cost, t);
+                        place(wcols_[r][t], wc, t);
             }
             if (!tuned_ || r == vd_ / 9) {
-                auto wr = runs(rows, rcost, rf, rc, kRunLength[r], cost);
+                auto wr = runs(rows, rcost, rf, rc, kRunLength[r]);
                 for (int t = 0; t < kCtaSizes; ++t)
                     if (!tuned_ || t == vd_ % 3)
-                        place(wrows_[r][t], wr, cost, t);
+                        place(wrows_[r][t], wr, t);
             }
         }
         ncols_ = int(cols.size());
