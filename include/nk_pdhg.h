@@ -122,8 +122,9 @@ nk_status nk_pdhg_stats(nk_pdhg *h, int64_t *trials, int64_t *device_bytes);
  * CUDA events around each kernel on the engine's stream and returns the mean
  * duration of the fused primal (A^T y + primal step) and dual (A dx + dual step
  * + decision) steps in milliseconds; the dual step includes the panel kernel
- * when A's long rows are stored by column panel.  The trials advance the
- * iterate. */
+ * when A's long rows are stored by column panel.  With graphs on, each trial
+ * replays one captured trial whose events are graph nodes, as the graph path
+ * runs it.  The trials advance the iterate. */
 nk_status nk_pdhg_profile(nk_pdhg *h, int count, double tau, double sigma, double *ms_primal,
                           double *ms_dual);
 /* The same, kernel by kernel: ms[0] the primal kernel, ms[1] the panel kernel

@@ -483,6 +483,7 @@ struct Engine {
     // per-kernel timing hooks: when set, events are recorded around the primal
     // and dual launches of each trial (profiling mode, no graphs)
     cudaEvent_t ev[4] = {};
+    bool ev_in_graph = false; // profile(): the events are recorded inside a captured trial
 
     ~Engine() {
         if (stream)
@@ -536,6 +537,14 @@ struct Engine {
     }
 
     // -------------------------------------------------------------- launches
+    // profiling event i after the preceding launch (inside a capture, as an
+    // external node, so that replaying the graph records it)
+    void mark(int i) {
+        cuda_check(cudaEventRecordWithFlags(ev[i], stream,
+                                            ev_in_graph ? cudaEventRecordExternal
+                                                        : cudaEventRecordDefault),
+                   "profile event");
+    }
     template <class Acc, class V, class I> void launch_trial_t() {
         Vecs v = vecs();
         constexpr bool F32 = sizeof(Acc) == 4;
@@ -543,11 +552,11 @@ struct Engine {
         auto a = A.fused_view<V, I>();
         auto qm = Q.view<V, I>();
         if (ev[0])
-            cudaEventRecord(ev[0], stream);
+            mark(0);
         primal_kernel_for<Acc, V, I>(sparse_q, At.nsv > 0)<<<grid_p, kFusedThreads, smem_p(),
                                                               stream>>>(at, qm, v);
         if (ev[1])
-            cudaEventRecord(ev[1], stream);
+            mark(1);
         if (panels) {
             using X = typename std::conditional<F32, float, double>::type;
             const X *dxp;
@@ -558,7 +567,7 @@ struct Engine {
             panel_kernel<Acc, V, X><<<pan.grid, kPanelThreads, pan.smem, stream>>>(
                 pan.view<V>(), dxp, ctl.p);
             if (ev[3])
-                cudaEventRecord(ev[3], stream);
+                mark(3);
             dual_kernel<Acc, V, I, F32, false, true><<<grid_d, kFusedThreads, smem_d(), stream>>>(a,
                                                                                                 v);
         } else if (A.nsv > 0)
@@ -566,7 +575,7 @@ struct Engine {
         else
             dual_kernel<Acc, V, I, F32, false><<<grid_d, kFusedThreads, smem_d(), stream>>>(a, v);
         if (ev[2])
-            cudaEventRecord(ev[2], stream);
+            mark(2);
         if (halpern)
             halpern_commit<<<grid_for(std::max(n, m)), kThreads, 0, stream>>>(n, m, v, F32);
     }
@@ -980,7 +989,9 @@ struct Engine {
     // Runs `count` trials one by one with events around each kernel; returns the
     // mean durations in milliseconds of the primal kernel, of the dual step (the
     // panel kernel, when A has panels, plus the dual kernel) and of the panel
-    // kernel alone (0 without panels).
+    // kernel alone (0 without panels).  With graphs on, each trial is a replay
+    // of one captured trial whose events are graph nodes, so the kernels run
+    // back to back as in the graph path; without, launches are plain.
     void profile(int count, double tau, double sigma, double *ms_primal, double *ms_dual,
                  double *ms_panel = nullptr) {
         if (count <= 0)
@@ -992,9 +1003,34 @@ struct Engine {
         for (auto &e : ev)
             cuda_check(cudaEventCreate(&e), "event");
         double tp = 0, td = 0, tk = 0;
+        cudaGraphExec_t one = nullptr;
         try {
+            if (graphs) {
+                // the trial as the graph path runs it: one captured trial with
+                // the events as graph nodes, replayed `count` times
+                cudaGraph_t g = nullptr;
+                ev_in_graph = true;
+                cuda_check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal),
+                           "profile capture");
+                try {
+                    launch_trial();
+                } catch (...) {
+                    cudaStreamEndCapture(stream, &g);
+                    if (g)
+                        cudaGraphDestroy(g);
+                    throw;
+                }
+                ev_in_graph = false;
+                cuda_check(cudaStreamEndCapture(stream, &g), "profile capture");
+                cudaError_t e = cudaGraphInstantiate(&one, g, 0);
+                cudaGraphDestroy(g);
+                cuda_check(e, "profile instantiate");
+            }
             for (int t = 0; t < count; ++t) {
-                launch_trial();
+                if (one)
+                    cuda_check(cudaGraphLaunch(one, stream), "profile launch");
+                else
+                    launch_trial();
                 cuda_check(cudaEventSynchronize(ev[2]), "profile sync");
                 float a = 0, b = 0, k = 0;
                 cudaEventElapsedTime(&a, ev[0], ev[1]);
@@ -1006,12 +1042,17 @@ struct Engine {
                 tk += k;
             }
         } catch (...) {
+            ev_in_graph = false;
+            if (one)
+                cudaGraphExecDestroy(one);
             for (auto &e : ev) {
                 cudaEventDestroy(e);
                 e = nullptr;
             }
             throw;
         }
+        if (one)
+            cudaGraphExecDestroy(one);
         for (auto &e : ev) {
             cudaEventDestroy(e);
             e = nullptr;

@@ -479,3 +479,21 @@ def test_trajectory_parity_above_openmp_threshold(gpu, reference):
         assert g.rejected_steps() == cpu.rejected_steps()
         for u, w in zip(g.candidates(), cpu.candidates()):
             near(u, w, 1e-8)
+
+
+@pytest.mark.parametrize("graphs", [False, True])
+def test_profiled_trials_are_ordinary_trials(gpu, graphs):
+    """nk_pdhg_profile_kernels times the kernels of real trials (with graphs on,
+    replays of one captured trial whose events are graph nodes): its trials
+    advance the iterate bit for bit as advance() does, and every kernel time is
+    positive, the panel kernel's too on an LP with panels."""
+    m = synth.power_law_lp(m=20000, n=100000, nnz=500000, seed=3, len_hi=5000)
+    tau, sigma = step_sizes(m)
+    a = gpu.PdhgBackend(m, adaptive=True, graphs=graphs)
+    b = gpu.PdhgBackend(m, adaptive=True, graphs=graphs)
+    assert a.layout_info()["panels"] >= 2
+    primal, panel, dual = a.profile_kernels(30, tau, sigma)
+    assert primal > 0 and panel > 0 and dual > 0
+    b.advance(30, tau, sigma)
+    for u, w in zip(a.candidates(), b.candidates()):
+        assert np.array_equal(u, w)
