@@ -48,11 +48,11 @@ struct BCtl { // per instance; the first fields mirror Control (nk_device.cuh)
 // Work item of the trial kernels: a run of `count` consecutive chunks of one
 // instance starting at `chunk`, whose partial sums go to part, part+1, ...
 // (partials are instance-contiguous).  A run shares one descriptor fetch.
-// Items are placed on CTAs on the host by estimated memory work (sorted
-// costliest first and dealt one per CTA per round, alternating direction;
-// CTA b owns list entries [coff[b], coff[b+1]), costliest first), and a CTA's
-// warps claim its items from a shared counter, so every SM finishes its share
-// at about the same time.
+// Items are placed on CTAs on the host by estimated memory work (runs of
+// consecutive items of equal work, a few per CTA; CTA b owns list entries
+// [coff[b], coff[b+1]), in instance and chunk order), and a CTA's warps claim
+// its items from a shared counter, so every SM finishes its share at about
+// the same time.
 // Where an item runs changes no result: its partials have fixed slots.
 struct BWork {
     int inst, chunk, part, count;
