@@ -820,40 +820,69 @@ class Batch {
                 }
             return items;
         };
-        // Items onto a resident grid of CTAs of size t.  The items, in instance
-        // and chunk order, are cut into kSegments * G consecutive segments of
-        // equal estimated work, and segment s goes to CTA s mod G.  A CTA's
-        // warps then work on a few runs of one instance's consecutive chunks at
-        // a time, gathering from the same x or dx lines in L1, while each CTA's
-        // share mixes instances from across the batch, so that errors of the
-        // cost estimate even out.  On the 512-instance batch an FP64 trial
-        // took 0.846 ms so, against 1.007 ms with all items sorted by cost and
+        // Items onto a resident grid of CTAs of size t.  With many instances
+        // (kSegmentInstances or more) the items, in instance and chunk order,
+        // are cut into kSegments * G consecutive segments of equal estimated
+        // work, and segment s goes to CTA s mod G.  A CTA's warps then work on
+        // a few runs of one instance's consecutive chunks at a time, gathering
+        // from the same x or dx lines in L1, while each CTA's share mixes
+        // instances from across the batch, so that errors of the cost
+        // estimate even out.  On the 512-instance batch an FP64 trial took
+        // 0.846 ms so, against 1.007 ms with all items sorted by cost and
         // dealt one per CTA in turn, 0.909 ms with one segment per CTA for the
-        // rows (columns dealt), and 0.871 ms with two per CTA for both.
-        constexpr int kSegments = 4;
+        // rows (columns dealt), and 0.871 ms with two per CTA for both.  With
+        // fewer instances the segments are too coarse to even out the
+        // estimate's errors (128 instances: 0.236 ms against 0.229 ms dealt),
+        // and the items are sorted by cost, costliest first (a stable counting
+        // sort), and dealt one per CTA per round, alternating direction (round
+        // k to CTAs 0..G-1 when k is even, G-1..0 when odd).
+        constexpr int kSegments = 4, kSegmentInstances = 256;
+        const bool segmented = int(order_.size()) >= kSegmentInstances;
         auto place = [&](WorkList &W, const std::vector<BWork> &items,
                          const std::vector<int64_t> &icost, int t) {
             const int ncta = std::max(1, std::min<int>(int(items.size()), sms_ * resident_[t]));
             std::vector<int> owner(items.size());
             std::vector<int> coff(size_t(ncta + 1), 0);
-            double total = 0;
-            for (int64_t c : icost)
-                total += double(c);
-            const int nseg = kSegments * ncta;
-            const double share = std::max(1e-9, total / nseg);
-            double before = 0;
-            for (size_t k = 0; k < items.size(); ++k) {
-                const int seg = std::min(nseg - 1, int((before + 0.5 * double(icost[k])) / share));
-                owner[k] = seg % ncta;
-                before += double(icost[k]);
-                ++coff[size_t(owner[k] + 1)];
+            std::vector<size_t> seq(items.size()); // the order the lists are filled in
+            std::iota(seq.begin(), seq.end(), size_t(0));
+            if (segmented) {
+                double total = 0;
+                for (int64_t c : icost)
+                    total += double(c);
+                const int nseg = kSegments * ncta;
+                const double share = std::max(1e-9, total / nseg);
+                double before = 0;
+                for (size_t k = 0; k < items.size(); ++k) {
+                    const int seg =
+                        std::min(nseg - 1, int((before + 0.5 * double(icost[k])) / share));
+                    owner[k] = seg % ncta;
+                    before += double(icost[k]);
+                    ++coff[size_t(owner[k] + 1)];
+                }
+            } else {
+                int64_t top = 0;
+                for (int64_t c : icost)
+                    top = std::max(top, c);
+                std::vector<int64_t> start(size_t(top + 2), 0);
+                for (int64_t c : icost)
+                    ++start[size_t(top - c + 1)];
+                for (size_t b = 1; b < start.size(); ++b)
+                    start[b] += start[b - 1];
+                for (size_t k = 0; k < items.size(); ++k)
+                    seq[size_t(start[size_t(top - icost[k])]++)] = k;
+                for (size_t r = 0; r < seq.size(); ++r) {
+                    const int round = int(r / size_t(ncta)), at = int(r % size_t(ncta));
+                    owner[seq[r]] = round % 2 ? ncta - 1 - at : at;
+                    ++coff[size_t(owner[seq[r]] + 1)];
+                }
             }
             for (int b = 0; b < ncta; ++b)
                 coff[size_t(b + 1)] += coff[size_t(b)];
-            // each CTA's list keeps instance and chunk order
+            // each CTA's list: in instance and chunk order (segments) or
+            // costliest first (dealt)
             std::vector<BWork> out(std::max<size_t>(1, items.size()));
             std::vector<int> fill(coff.begin(), coff.end() - 1);
-            for (size_t k = 0; k < items.size(); ++k)
+            for (size_t k : seq)
                 out[size_t(fill[size_t(owner[k])]++)] = items[k];
             ensure(W.items, out.size());
             ensure(W.coff, coff.size());
