@@ -831,12 +831,13 @@ class Batch {
         // 0.846 ms so, against 1.007 ms with all items sorted by cost and
         // dealt one per CTA in turn, 0.909 ms with one segment per CTA for the
         // rows (columns dealt), and 0.871 ms with two per CTA for both.  With
-        // fewer instances the segments are too coarse to even out the
-        // estimate's errors (128 instances: 0.236 ms against 0.229 ms dealt),
-        // and the items are sorted by cost, costliest first (a stable counting
+        // few instances a CTA's segments come from one or two instances and
+        // the estimate's errors no longer even out (the served stream, about
+        // 45 active instances: 115 requests completed against 135 dealt), and
+        // the items are sorted by cost, costliest first (a stable counting
         // sort), and dealt one per CTA per round, alternating direction (round
         // k to CTAs 0..G-1 when k is even, G-1..0 when odd).
-        constexpr int kSegments = 4, kSegmentInstances = 256;
+        constexpr int kSegments = 4, kSegmentInstances = 64;
         const bool segmented = int(order_.size()) >= kSegmentInstances;
         auto place = [&](WorkList &W, const std::vector<BWork> &items,
                          const std::vector<int64_t> &icost, int t) {
