@@ -100,3 +100,18 @@ def test_invalid_options_are_refused():
         _prepare(lp, check_every=0)
     with pytest.raises(ValueError, match="fp64 or mixed"):
         batch.batch_options(matrix_precision="fp32")
+
+
+def test_precision_defaults():
+    """The batch's C default and its Python default are FP64 matrices; the
+    served stream's default is MIXED (each chosen by certified solves per
+    second on its own workload)."""
+    import inspect
+    from niryukti_b200 import serve
+    L = _lib()
+    o = batch.NkBatchOptions()
+    L.nk_batch_defaults(C.byref(o))
+    assert o.precision == batch.PRECISIONS["fp64"]
+    assert batch.batch_options().precision == batch.PRECISIONS["fp64"]
+    sig = inspect.signature(serve.SolveService.__init__)
+    assert sig.parameters["matrix_precision"].default == "mixed"
